@@ -1,0 +1,231 @@
+/*
+ * tg2dgs.h -- C ABI of the B200 textured 2DGS rasterization path.
+ *
+ * Plain pointers and sizes only.  Every buffer (inputs, outputs, workspace) is
+ * allocated and owned by the caller; every entry point enqueues work on the
+ * given CUDA stream and returns 0 on success or a negative TG_ERR_* code (the
+ * message is available from tg_last_error()).  Entry points are safe to call
+ * concurrently from several host threads on distinct streams.
+ *
+ * Each entry point names the reference interface it replaces (paths inside the
+ * Camak2441/textured_gaussians project).
+ */
+#ifndef TG2DGS_H
+#define TG2DGS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* tg_stream_t; /* same type as cudaStream_t */
+
+#if defined(__GNUC__)
+#define TG_API __attribute__((visibility("default")))
+#else
+#define TG_API
+#endif
+
+#define TG_OK 0
+#define TG_ERR_INVALID_ARG (-1)   /* null pointer, bad size, misaligned buffer */
+#define TG_ERR_UNSUPPORTED (-2)   /* channel count / texture format / tile size not supported */
+#define TG_ERR_CUDA (-3)          /* a CUDA launch or runtime call failed */
+#define TG_ERR_WORKSPACE (-4)     /* workspace smaller than tg_sort_workspace_bytes() */
+#define TG_ERR_TIMEOUT (-5)       /* a bounded device-side wait gave up */
+
+/* texture storage formats (textures are [G, ry, rx, 4] RGBA texels) */
+#define TG_TEX_NONE 0  /* plain 2DGS compositor, no textures */
+#define TG_TEX_F32 1
+#define TG_TEX_BF16 2
+#define TG_TEX_F16 3
+#define TG_TEX_FP8_E4M3 4 /* plus one float scale per Gaussian: texel = fp8 * scale */
+
+/* compositor adjoint forms */
+#define TG_ADJ_REFERENCE 0 /* "bilinear": texture lookup not differentiated w.r.t. geometry */
+#define TG_ADJ_BWD2 1      /* "bilinear_bwd2": reference UV term (du/ds factor (R-1)/range) */
+#define TG_ADJ_EXACT 2     /* exact derivative of the forward ((R-1)/(2*range)) */
+
+TG_API int tg_version(void);
+TG_API const char* tg_last_error(void);
+/* Number of kernels this library has launched in this process (all devices,
+ * all threads); lets a harness count the launches inside a timed region.
+ * No counterpart in the reference. */
+TG_API uint64_t tg_kernel_launch_count(void);
+
+/* ------------------------------------------------------------------ projection
+ * Replaces fully_fused_projection_fwd_2dgs_tensor
+ * (textured_gaussians/cuda/csrc/fully_fused_projection_2dgs_fwd.cu:247-304).
+ * All float arrays are FP32, row-major.  Entries that are culled get radii 0
+ * and zeros elsewhere. */
+typedef struct {
+    int32_t C, N;
+    const float* means;    /* [N,3] */
+    const float* quats;    /* [N,4] wxyz, not necessarily normalised */
+    const float* scales;   /* [N,3] (third unused) */
+    const float* viewmats; /* [C,4,4] world-to-camera */
+    const float* Ks;       /* [C,3,3] */
+    int32_t width, height;
+    float near_plane, far_plane, radius_clip;
+    int32_t* radii;        /* [C,N] */
+    float* means2d;        /* [C,N,2] */
+    float* depths;         /* [C,N] */
+    float* ray_transforms; /* [C,N,3,3] rows of K*[R*s0*q0, R*s1*q1, mean_c] */
+    float* normals;        /* [C,N,3] */
+} tg_project_fwd_args;
+TG_API int tg_project_fwd(const tg_project_fwd_args* a, tg_stream_t stream);
+
+/* Replaces fully_fused_projection_bwd_2dgs_tensor / fully_fused_projection_bwd2_2dgs_tensor
+ * (textured_gaussians/cuda/csrc/fully_fused_projection_2dgs_bwd.cu:150-222, ..._bwd2.cu).
+ * mode: 0 reference, 1 norm_rot_grad (bwd2), 2 exact.  v_means/v_quats/v_scales
+ * are overwritten (zeroed, then accumulated). */
+typedef struct {
+    int32_t C, N;
+    const float* means;
+    const float* quats;
+    const float* scales;
+    const float* viewmats;
+    const float* Ks;
+    const int32_t* radii;          /* [C,N] */
+    const float* ray_transforms;   /* [C,N,9] */
+    const float* v_means2d;        /* [C,N,2] */
+    const float* v_depths;         /* [C,N] */
+    const float* v_normals;        /* [C,N,3] */
+    const float* v_ray_transforms; /* [C,N,9] */
+    int32_t mode;
+    float* v_means;  /* [N,3] */
+    float* v_quats;  /* [N,4] */
+    float* v_scales; /* [N,3] */
+} tg_project_bwd_args;
+TG_API int tg_project_bwd(const tg_project_bwd_args* a, tg_stream_t stream);
+
+/* ------------------------------------------------------------------ tile intersection
+ * Replaces isect_tiles_tensor (textured_gaussians/cuda/csrc/isect_tiles.cu:107-307),
+ * split at the one host synchronisation the reference also has (:200-201):
+ * tg_isect_count writes tiles_per_gauss, the inclusive prefix sum cum_tiles and
+ * the total *n_isects (device scalar); tg_isect_emit then writes the unsorted
+ * keys cam<<(32+tile_bits) | tile<<32 | bits(depth) and flatten ids. */
+typedef struct {
+    int64_t n_elems;            /* C*N dense, nnz packed */
+    int64_t N;                  /* dense: Gaussians per camera; packed: 0 */
+    const int64_t* camera_ids;  /* packed: [nnz]; dense: NULL */
+    const float* means2d;       /* [n_elems,2] */
+    const int32_t* radii;       /* [n_elems] */
+    const float* depths;        /* [n_elems] */
+    int32_t tile_size, tile_width, tile_height, n_cameras;
+    int32_t* tiles_per_gauss;   /* [n_elems] */
+    int64_t* cum_tiles;         /* [n_elems] inclusive prefix sum */
+    int64_t* n_isects;          /* [1] device */
+    void* scan_workspace;       /* tg_scan_workspace_bytes(n_elems) bytes */
+    int64_t* isect_ids;         /* [n_isects] (emit only) */
+    int32_t* flatten_ids;       /* [n_isects] (emit only) */
+} tg_isect_args;
+TG_API size_t tg_scan_workspace_bytes(int64_t n_elems);
+TG_API int tg_isect_count(const tg_isect_args* a, tg_stream_t stream);
+TG_API int tg_isect_emit(const tg_isect_args* a, tg_stream_t stream);
+
+/* Stable LSD onesweep radix sort of (int64 key, int32 value) pairs on key bits
+ * [0, end_bit), ping-ponging between (keys, vals) and (keys_alt, vals_alt).
+ * Replaces cub::DeviceRadixSort::SortPairs as called at
+ * textured_gaussians/cuda/csrc/isect_tiles.cu:246-300.  *result_in_alt (host
+ * int) is set to 1 when the sorted data ends in the *_alt buffers. */
+TG_API size_t tg_sort_workspace_bytes(int64_t n, int32_t end_bit);
+TG_API int tg_sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, int64_t n, int32_t end_bit,
+                  void* workspace, size_t workspace_bytes, int32_t* result_in_alt, tg_stream_t stream);
+
+/* Replaces isect_offset_encode_tensor (textured_gaussians/cuda/csrc/isect_tiles.cu:357-390):
+ * offsets[c,ty,tx] = index of the first sorted intersection of tile (c,ty,tx)
+ * or of the next non-empty tile. */
+TG_API int tg_isect_offset_encode(const int64_t* isect_ids, int64_t n_isects, int32_t n_cameras, int32_t tile_width,
+                           int32_t tile_height, int32_t* offsets, tg_stream_t stream);
+
+/* ------------------------------------------------------------------ compositor
+ * Replaces rasterize_to_pixels_fwd_textured_gaussians_tensor
+ * (textured_gaussians/cuda/csrc/rasterize_to_pixels_textured_gaussians_2dgs_fwd.cu:618-690)
+ * and, with tex_format TG_TEX_NONE, rasterize_to_pixels_fwd_2dgs_tensor
+ * (textured_gaussians/cuda/csrc/rasterize_to_pixels_2dgs_fwd.cu:566-631).
+ * Element arrays are [E,...] with E = C*N (dense) or nnz (packed).  The
+ * texture row of element e is gaussian_ids[e] when gaussian_ids != NULL
+ * (packed) and e % N otherwise. */
+typedef struct {
+    int32_t C, N, D;            /* cameras, Gaussians, colour channels (1..5) */
+    int32_t width, height, tile_size, tile_width, tile_height;
+    int64_t n_isects;
+    const float* means2d;       /* [E,2] */
+    const float* ray_transforms;/* [E,9] */
+    const float* colors;        /* [E,D] */
+    const float* opacities;     /* [E] */
+    const float* normals;       /* [E,3] */
+    int32_t tex_format;         /* TG_TEX_* */
+    const void* textures;       /* [G,ry,rx,4] in tex_format */
+    const float* tex_scales;    /* [G] (fp8 only) */
+    int32_t tex_ry, tex_rx;
+    float range_x, range_y;
+    const float* backgrounds;   /* [C,D] or NULL */
+    const uint8_t* masks;       /* [C,tile_height,tile_width] or NULL */
+    const int32_t* tile_offsets;/* [C,tile_height,tile_width] */
+    const int32_t* flatten_ids; /* [n_isects] */
+    const int64_t* gaussian_ids;/* [E] or NULL */
+    float contrib_threshold, g_weight;
+    int32_t n_contrib;          /* length of contrib_sum/count (N, or G when packed) */
+    float* out_colors;          /* [C,H,W,D] */
+    float* out_alphas;          /* [C,H,W] */
+    float* out_normals;         /* [C,H,W,3] */
+    float* out_distort;         /* [C,H,W] */
+    float* out_median;          /* [C,H,W] */
+    int32_t* last_ids;          /* [C,H,W] */
+    int32_t* median_ids;        /* [C,H,W] */
+    float* contrib_sum;         /* [n_contrib] (zeroed by the call) */
+    float* contrib_count;       /* [n_contrib] (zeroed by the call) */
+} tg_raster_fwd_args;
+TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
+
+/* Replaces rasterize_to_pixels_bwd_textured_gaussians_tensor
+ * (textured_gaussians/cuda/csrc/rasterize_to_pixels_textured_gaussians_2dgs_bwd.cu:890-984),
+ * the bwd2 variant (..._bwd2.cu) and rasterize_to_pixels_bwd_2dgs_tensor
+ * (textured_gaussians/cuda/csrc/rasterize_to_pixels_2dgs_bwd.cu).  All
+ * gradient outputs are zeroed by the call, then accumulated.  v_densify is
+ * written after the accumulation completes. */
+typedef struct {
+    tg_raster_fwd_args f;        /* forward inputs (output pointers unused) */
+    const float* render_colors;  /* [C,H,W,D] forward outputs */
+    const float* render_alphas;  /* [C,H,W] */
+    const int32_t* last_ids;     /* [C,H,W] */
+    const int32_t* median_ids;   /* [C,H,W] */
+    const float* v_render_colors;  /* [C,H,W,D] */
+    const float* v_render_alphas;  /* [C,H,W] */
+    const float* v_render_normals; /* [C,H,W,3] */
+    const float* v_render_distort; /* [C,H,W] */
+    const float* v_render_median;  /* [C,H,W] */
+    int32_t adjoint;             /* TG_ADJ_* */
+    int64_t n_elems;             /* E */
+    float* v_means2d;            /* [E,2] */
+    float* v_means2d_abs;        /* [E,2] or NULL */
+    float* v_ray_transforms;     /* [E,9] */
+    float* v_colors;             /* [E,D] */
+    float* v_opacities;          /* [E] */
+    float* v_normals;            /* [E,3] */
+    float* v_textures;           /* [G,ry,rx,4] FP32 or NULL */
+    float* v_densify;            /* [E,2] */
+} tg_raster_bwd_args;
+TG_API int tg_rasterize_bwd(const tg_raster_bwd_args* a, tg_stream_t stream);
+
+/* ------------------------------------------------------------------ spherical harmonics
+ * Replaces compute_sh_fwd_tensor / compute_sh_bwd_tensor
+ * (textured_gaussians/cuda/csrc/compute_sh_fwd.cu, compute_sh_bwd.cu).
+ * colors[i,3] = sum_k basis_k(normalize(dirs[i])) coeffs[i % coeff_rows,k,:]
+ * for i < n; masked-out elements are written as zeros.  coeff_rows < n lets
+ * C cameras share one [N,K,3] coefficient table without materialising C
+ * copies (n = C*N, coeff_rows = N).  Backward overwrites v_coeffs
+ * ([coeff_rows,K,3], summed over the elements sharing a row, deterministic)
+ * and, if non-NULL, v_dirs ([n,3]). */
+TG_API int tg_sh_fwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, const float* dirs, const float* coeffs,
+                     const uint8_t* masks, float* colors, tg_stream_t stream);
+TG_API int tg_sh_bwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, const float* dirs, const float* coeffs,
+                     const uint8_t* masks, const float* v_colors, float* v_coeffs, float* v_dirs, tg_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TG2DGS_H */

@@ -1,0 +1,280 @@
+"""numpy front end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loads oracle/libtg_oracle.so (built by oracle/build.py) through ctypes and
+exposes the stages of the textured 2DGS path plus a whole-pipeline
+``render`` / ``render_backward`` pair that mirrors
+``rasterization_textured_gaussians`` (textured_gaussians/rendering.py:1474-1685)
+and ``rasterization_2dgs`` (textured_gaussians/rendering.py:1135-1338).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, and only as the checker.  The product package never does.
+
+Parity status: projection, intersection, offsets and SH are pinned against
+golden vectors from the reference's pure-torch twins; the plain compositor is
+pinned against the reference's torch ``accumulate_2dgs``; the textured
+compositor is a restatement with no executable reference ("parity unpinned").
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import build as _build
+
+_LIB = None
+
+c_int = ctypes.c_int
+c_i64 = ctypes.c_int64
+c_dbl = ctypes.c_double
+c_ptr = ctypes.c_void_p
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = _build.build()
+        _LIB = ctypes.CDLL(path)
+        for suf in ("f32", "f64"):
+            getattr(_LIB, f"tgo_project_fwd_{suf}").argtypes = [c_int, c_int] + [c_ptr] * 5 + [c_int, c_int, c_dbl, c_dbl, c_dbl] + [c_ptr] * 5
+            getattr(_LIB, f"tgo_project_bwd_{suf}").argtypes = [c_int, c_int] + [c_ptr] * 11 + [c_int] + [c_ptr] * 3
+            getattr(_LIB, f"tgo_isect_count_{suf}").argtypes = [c_i64, c_ptr, c_ptr, c_int, c_int, c_int, c_ptr]
+            getattr(_LIB, f"tgo_isect_emit_{suf}").argtypes = [c_i64, c_i64] + [c_ptr] * 5 + [c_int] * 4 + [c_ptr] * 2
+            getattr(_LIB, f"tgo_sh_fwd_{suf}").argtypes = [c_i64, c_int, c_int] + [c_ptr] * 4
+            getattr(_LIB, f"tgo_sh_bwd_{suf}").argtypes = [c_i64, c_int, c_int] + [c_ptr] * 6
+            getattr(_LIB, f"tgo_raster_fwd_{suf}").argtypes = (
+                [c_int] * 8 + [c_i64] + [c_ptr] * 6 + [c_int, c_int, c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl, c_dbl] + [c_ptr] * 11
+            )
+            getattr(_LIB, f"tgo_raster_bwd_{suf}").argtypes = (
+                [c_int] * 8 + [c_i64, c_i64] + [c_ptr] * 6 + [c_int, c_int, c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl]
+                + [c_ptr] * 9 + [c_int] + [c_ptr] * 8
+            )
+        _LIB.tgo_sort_pairs.argtypes = [c_i64, c_ptr, c_ptr, c_int]
+        _LIB.tgo_offset_encode.argtypes = [c_i64, c_ptr, c_int, c_int, c_int, c_ptr]
+    return _LIB
+
+
+def _p(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be C-contiguous"
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _suf(dtype) -> str:
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+def _c(a, dtype):
+    return None if a is None else np.ascontiguousarray(a, dtype=dtype)
+
+
+def tile_bits(n: int) -> int:
+    """floor(log2(n)) + 1, the bit width the reference uses (isect_tiles.cu:156-157)."""
+    return int(math.floor(math.log2(n))) + 1
+
+
+# ------------------------------------------------------------------ projection
+def project_fwd(means, quats, scales, viewmats, Ks, W, H, near_plane=0.01, far_plane=1e10, radius_clip=0.0,
+                dtype=np.float32):
+    means, quats, scales, viewmats, Ks = (_c(x, dtype) for x in (means, quats, scales, viewmats, Ks))
+    C, N = viewmats.shape[0], means.shape[0]
+    radii = np.zeros((C, N), np.int32)
+    means2d = np.zeros((C, N, 2), dtype)
+    depths = np.zeros((C, N), dtype)
+    M = np.zeros((C, N, 3, 3), dtype)
+    normals = np.zeros((C, N, 3), dtype)
+    getattr(lib(), f"tgo_project_fwd_{_suf(dtype)}")(
+        C, N, _p(means), _p(quats), _p(scales), _p(viewmats), _p(Ks), int(W), int(H), near_plane, far_plane,
+        radius_clip, _p(radii), _p(means2d), _p(depths), _p(M), _p(normals))
+    return radii, means2d, depths, M, normals
+
+
+def project_bwd(means, quats, scales, viewmats, Ks, radii, M, v_means2d, v_depths, v_normals, v_M, mode=0,
+                dtype=np.float32):
+    """mode 0: reference adjoint, 1: reference norm_rot_grad adjoint, 2: exact."""
+    args = [_c(x, dtype) for x in (means, quats, scales, viewmats, Ks)]
+    C, N = args[3].shape[0], args[0].shape[0]
+    radii = np.ascontiguousarray(radii, np.int32)
+    rest = [_c(x, dtype) for x in (M, v_means2d, v_depths, v_normals, v_M)]
+    v_means = np.zeros((N, 3), dtype)
+    v_quats = np.zeros((N, 4), dtype)
+    v_scales = np.zeros((N, 3), dtype)
+    getattr(lib(), f"tgo_project_bwd_{_suf(dtype)}")(
+        C, N, *[_p(x) for x in args], _p(radii), *[_p(x) for x in rest], int(mode), _p(v_means), _p(v_quats),
+        _p(v_scales))
+    return v_means, v_quats, v_scales
+
+
+# ------------------------------------------------------------------ intersection
+def isect_tiles(means2d, radii, depths, tile_size, tile_width, tile_height, n_cameras, camera_ids=None,
+                sort=True):
+    """Tile counts, 64-bit keys and flatten ids; sorted stably on the reference's bit range."""
+    fdt = np.float64 if np.asarray(means2d).dtype == np.float64 else np.float32
+    means2d = np.ascontiguousarray(means2d, fdt)
+    radii = np.ascontiguousarray(radii, np.int32)
+    depths32 = np.ascontiguousarray(depths, np.float32)
+    packed = means2d.ndim == 2
+    E = means2d.shape[0] if packed else means2d.shape[0] * means2d.shape[1]
+    N = 0 if packed else means2d.shape[1]
+    tpg = np.zeros(radii.shape, np.int32)
+    L = lib()
+    getattr(L, f"tgo_isect_count_{_suf(fdt)}")(E, _p(means2d), _p(radii), tile_size, tile_width, tile_height, _p(tpg))
+    cum = np.cumsum(tpg.reshape(-1).astype(np.int64))
+    n_isects = int(cum[-1]) if E else 0
+    isect_ids = np.zeros(n_isects, np.int64)
+    flatten_ids = np.zeros(n_isects, np.int32)
+    tb = tile_bits(tile_width * tile_height)
+    cb = tile_bits(n_cameras)
+    cam = None if camera_ids is None else np.ascontiguousarray(camera_ids, np.int64)
+    if n_isects:
+        getattr(L, f"tgo_isect_emit_{_suf(fdt)}")(E, N, _p(cam), _p(means2d), _p(radii), _p(depths32), _p(cum),
+                                                   tile_size, tile_width, tile_height, tb, _p(isect_ids),
+                                                   _p(flatten_ids))
+        if sort:
+            L.tgo_sort_pairs(n_isects, _p(isect_ids), _p(flatten_ids), 32 + tb + cb)
+    return tpg, isect_ids, flatten_ids
+
+
+def sort_pairs(keys, vals, end_bit):
+    keys = np.array(keys, np.int64, copy=True)
+    vals = np.array(vals, np.int32, copy=True)
+    lib().tgo_sort_pairs(keys.size, _p(keys), _p(vals), int(end_bit))
+    return keys, vals
+
+
+def isect_offset_encode(isect_ids, n_cameras, tile_width, tile_height):
+    isect_ids = np.ascontiguousarray(isect_ids, np.int64)
+    n_tiles = tile_width * tile_height
+    offsets = np.zeros((n_cameras, tile_height, tile_width), np.int32)
+    lib().tgo_offset_encode(isect_ids.size, _p(isect_ids), n_cameras, n_tiles, tile_bits(n_tiles), _p(offsets))
+    return offsets
+
+
+# ------------------------------------------------------------------ SH
+def sh_fwd(degree, dirs, coeffs, masks=None, dtype=np.float32):
+    dirs = _c(dirs, dtype)
+    lead = dirs.shape[:-1]
+    coeffs = _c(np.broadcast_to(coeffs, lead + coeffs.shape[-2:]), dtype)
+    n = int(np.prod(lead))
+    K = coeffs.shape[-2]
+    m = None if masks is None else np.ascontiguousarray(np.broadcast_to(masks, lead), np.uint8)
+    out = np.zeros(lead + (3,), dtype)
+    getattr(lib(), f"tgo_sh_fwd_{_suf(dtype)}")(n, degree, K, _p(dirs), _p(coeffs), _p(m), _p(out))
+    return out
+
+
+def sh_bwd(degree, dirs, coeffs, v_colors, masks=None, dtype=np.float32):
+    dirs = _c(dirs, dtype)
+    lead = dirs.shape[:-1]
+    coeffs = _c(np.broadcast_to(coeffs, lead + coeffs.shape[-2:]), dtype)
+    n = int(np.prod(lead))
+    K = coeffs.shape[-2]
+    m = None if masks is None else np.ascontiguousarray(np.broadcast_to(masks, lead), np.uint8)
+    v_colors = _c(v_colors, dtype)
+    v_coeffs = np.zeros_like(coeffs)
+    v_dirs = np.zeros_like(dirs)
+    getattr(lib(), f"tgo_sh_bwd_{_suf(dtype)}")(n, degree, K, _p(dirs), _p(coeffs), _p(m), _p(v_colors),
+                                                _p(v_coeffs), _p(v_dirs))
+    return v_coeffs, v_dirs
+
+
+# ------------------------------------------------------------------ compositor
+@dataclass
+class RasterFwdOut:
+    colors: np.ndarray
+    alphas: np.ndarray
+    normals: np.ndarray
+    distort: np.ndarray
+    median: np.ndarray
+    last_ids: np.ndarray
+    median_ids: np.ndarray
+    contrib_sum: np.ndarray
+    contrib_count: np.ndarray
+    pair_count: np.ndarray
+    branch_sig: np.ndarray
+
+
+def raster_fwd(means2d, M, colors, opacities, normals, textures, offsets, flatten_ids, W, H, tile_size,
+               range_x=3.0, range_y=3.0, backgrounds=None, masks=None, gaussian_ids=None, n_gauss=None,
+               contrib_threshold=0.0, g_weight=1.0, dtype=np.float32):
+    """Compositor forward.  ``textures=None`` selects the plain 2DGS compositor.
+
+    Dense layout: means2d [C,N,2] ...; packed layout: [nnz,...] plus
+    ``gaussian_ids`` [nnz] and ``n_gauss``.
+    """
+    means2d, M, colors, opacities, normals, textures, backgrounds = (
+        _c(x, dtype) for x in (means2d, M, colors, opacities, normals, textures, backgrounds))
+    offsets = np.ascontiguousarray(offsets, np.int32)
+    flatten_ids = np.ascontiguousarray(flatten_ids, np.int32)
+    C, th, tw = offsets.shape
+    packed = means2d.ndim == 2
+    N = n_gauss if packed else means2d.shape[1]
+    D = colors.shape[-1]
+    G = N if gaussian_ids is None else n_gauss
+    gid = None if gaussian_ids is None else np.ascontiguousarray(gaussian_ids, np.int64)
+    m = None if masks is None else np.ascontiguousarray(masks, np.uint8)
+    ry, rx = (textures.shape[1], textures.shape[2]) if textures is not None else (0, 0)
+    o = RasterFwdOut(
+        colors=np.zeros((C, H, W, D), dtype), alphas=np.zeros((C, H, W, 1), dtype), normals=np.zeros((C, H, W, 3), dtype),
+        distort=np.zeros((C, H, W, 1), dtype), median=np.zeros((C, H, W, 1), dtype),
+        last_ids=np.zeros((C, H, W), np.int32), median_ids=np.zeros((C, H, W), np.int32),
+        contrib_sum=np.zeros((G,), dtype), contrib_count=np.zeros((G,), dtype), pair_count=np.zeros((C, H, W), np.int32),
+        branch_sig=np.zeros((C, H, W), np.uint64))
+    getattr(lib(), f"tgo_raster_fwd_{_suf(dtype)}")(
+        C, N, D, int(W), int(H), tile_size, tw, th, flatten_ids.size, _p(means2d), _p(M), _p(colors), _p(opacities),
+        _p(normals), _p(textures), ry, rx, float(range_x), float(range_y), _p(backgrounds), _p(m), _p(offsets),
+        _p(flatten_ids), _p(gid), float(contrib_threshold), float(g_weight), _p(o.colors), _p(o.alphas),
+        _p(o.normals), _p(o.distort), _p(o.median), _p(o.last_ids), _p(o.median_ids), _p(o.contrib_sum),
+        _p(o.contrib_count), _p(o.pair_count), _p(o.branch_sig))
+    return o
+
+
+@dataclass
+class RasterBwdOut:
+    v_means2d: np.ndarray
+    v_means2d_abs: np.ndarray
+    v_M: np.ndarray
+    v_colors: np.ndarray
+    v_opacities: np.ndarray
+    v_normals: np.ndarray
+    v_textures: Optional[np.ndarray]
+    v_densify: np.ndarray
+
+
+def raster_bwd(means2d, M, colors, opacities, normals, textures, offsets, flatten_ids, W, H, tile_size, fwd,
+               v_colors, v_alphas, v_normals, v_distort, v_median, range_x=3.0, range_y=3.0, backgrounds=None,
+               masks=None, gaussian_ids=None, n_gauss=None, g_weight=1.0, mode=0, dtype=np.float32):
+    """Compositor adjoint.  mode 0: reference "bilinear", 1: "bilinear_bwd2", 2: exact."""
+    means2d, M, colors, opacities, normals, textures, backgrounds = (
+        _c(x, dtype) for x in (means2d, M, colors, opacities, normals, textures, backgrounds))
+    offsets = np.ascontiguousarray(offsets, np.int32)
+    flatten_ids = np.ascontiguousarray(flatten_ids, np.int32)
+    C, th, tw = offsets.shape
+    packed = means2d.ndim == 2
+    N = n_gauss if packed else means2d.shape[1]
+    D = colors.shape[-1]
+    E = means2d.shape[0] if packed else C * N
+    gid = None if gaussian_ids is None else np.ascontiguousarray(gaussian_ids, np.int64)
+    m = None if masks is None else np.ascontiguousarray(masks, np.uint8)
+    ry, rx = (textures.shape[1], textures.shape[2]) if textures is not None else (0, 0)
+    fc, fa = _c(fwd.colors, dtype), _c(fwd.alphas, dtype)
+    li, mi = np.ascontiguousarray(fwd.last_ids, np.int32), np.ascontiguousarray(fwd.median_ids, np.int32)
+    vc, va, vn, vd, vm = (_c(x, dtype) for x in (v_colors, v_alphas, v_normals, v_distort, v_median))
+    o = RasterBwdOut(
+        v_means2d=np.zeros(means2d.shape, dtype), v_means2d_abs=np.zeros(means2d.shape, dtype),
+        v_M=np.zeros(M.shape, dtype), v_colors=np.zeros(colors.shape, dtype),
+        v_opacities=np.zeros(opacities.shape, dtype), v_normals=np.zeros(normals.shape, dtype),
+        v_textures=None if textures is None else np.zeros(textures.shape, dtype),
+        v_densify=np.zeros(means2d.shape, dtype))
+    getattr(lib(), f"tgo_raster_bwd_{_suf(dtype)}")(
+        C, N, D, int(W), int(H), tile_size, tw, th, flatten_ids.size, E, _p(means2d), _p(M), _p(colors),
+        _p(opacities), _p(normals), _p(textures), ry, rx, float(range_x), float(range_y), _p(backgrounds), _p(m),
+        _p(offsets), _p(flatten_ids), _p(gid), float(g_weight), _p(fc), _p(fa), _p(li), _p(mi), _p(vc), _p(va),
+        _p(vn), _p(vd), _p(vm), int(mode), _p(o.v_means2d), _p(o.v_means2d_abs), _p(o.v_M), _p(o.v_colors),
+        _p(o.v_opacities), _p(o.v_normals), _p(o.v_textures), _p(o.v_densify))
+    return o

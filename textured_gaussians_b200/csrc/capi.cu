@@ -1,0 +1,270 @@
+// extern "C" entry points of libtg2dgs.so (declared in include/tg2dgs.h).
+//
+// Each entry point validates its arguments (null pointers, sizes, alignment of
+// vector-loaded buffers, supported channel counts / formats / tile sizes),
+// enqueues its kernels on the caller's stream and maps failures to TG_ERR_*
+// codes with a per-thread message.  Nothing here allocates device memory:
+// every buffer, including scratch workspaces, comes from the caller.
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "tg_common.cuh"
+
+namespace tg {
+cudaError_t launch_project_fwd(const tg_project_fwd_args& a, cudaStream_t s);
+cudaError_t launch_project_bwd(const tg_project_bwd_args& a, cudaStream_t s);
+size_t scan_workspace_bytes(int64_t n_elems);
+cudaError_t launch_isect_count(const tg_isect_args& a, cudaStream_t s);
+cudaError_t launch_isect_emit(const tg_isect_args& a, int tile_n_bits, cudaStream_t s);
+size_t sort_workspace_bytes(int64_t n, int end_bit);
+int sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, int64_t n, int end_bit,
+               void* workspace, size_t ws_bytes, int32_t* result_in_alt, cudaStream_t s, cudaError_t& cerr);
+cudaError_t launch_offset_encode(const int64_t* keys, int64_t n, int C, int tw, int th, int tile_n_bits, int end_bit,
+                                 int32_t* offsets, cudaStream_t s);
+cudaError_t launch_raster_fwd(const tg_raster_fwd_args& a, cudaStream_t s);
+cudaError_t launch_raster_bwd(const tg_raster_bwd_args& a, cudaStream_t s);
+cudaError_t launch_sh_fwd(int64_t n, int64_t rows, int degree, int K, const float* dirs, const float* coeffs,
+                          const uint8_t* masks, float* colors, cudaStream_t s);
+cudaError_t launch_sh_bwd(int64_t n, int64_t rows, int degree, int K, const float* dirs, const float* coeffs,
+                          const uint8_t* masks, const float* v_colors, float* v_coeffs, float* v_dirs,
+                          cudaStream_t s);
+}  // namespace tg
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}  // namespace
+void tg::note_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_status(cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return TG_OK;
+    return fail(TG_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+int bit_width(int64_t n) {  // floor(log2(n)) + 1, as the reference computes it
+    int b = 0;
+    while (n > 0) { ++b; n >>= 1; }
+    return b;
+}
+
+#define TG_REQUIRE(cond, code, ...) \
+    do {                            \
+        if (!(cond)) return fail(code, __VA_ARGS__); \
+    } while (0)
+
+int check_raster_common(const tg_raster_fwd_args& a) {
+    TG_REQUIRE(a.C >= 0 && a.width >= 0 && a.height >= 0, TG_ERR_INVALID_ARG, "negative sizes");
+    TG_REQUIRE(a.tile_size == 16 || a.tile_size == 8, TG_ERR_UNSUPPORTED, "tile_size %d not supported (8 or 16)",
+               a.tile_size);
+    TG_REQUIRE(a.D >= 1 && a.D <= 5, TG_ERR_UNSUPPORTED, "unsupported number of channels: %d", a.D);
+    TG_REQUIRE((int64_t)a.tile_width * a.tile_size >= a.width && (int64_t)a.tile_height * a.tile_size >= a.height,
+               TG_ERR_INVALID_ARG, "tile grid %dx%d does not cover the image", a.tile_width, a.tile_height);
+    TG_REQUIRE(a.n_isects >= 0 && a.n_isects < (int64_t(1) << 31), TG_ERR_INVALID_ARG, "n_isects out of range");
+    TG_REQUIRE(a.tile_offsets && (a.n_isects == 0 || a.flatten_ids), TG_ERR_INVALID_ARG, "null offsets/flatten ids");
+    TG_REQUIRE(a.means2d && a.ray_transforms && a.colors && a.opacities && a.normals, TG_ERR_INVALID_ARG,
+               "null splat array");
+    TG_REQUIRE(aligned(a.means2d, 8), TG_ERR_INVALID_ARG, "means2d must be 8-byte aligned");
+    TG_REQUIRE(a.gaussian_ids != nullptr || a.N > 0 || a.n_isects == 0, TG_ERR_INVALID_ARG, "N must be > 0");
+    switch (a.tex_format) {
+        case TG_TEX_NONE: break;
+        case TG_TEX_F32:
+            TG_REQUIRE(a.textures && aligned(a.textures, 16), TG_ERR_INVALID_ARG, "FP32 textures must be 16-byte aligned");
+            break;
+        case TG_TEX_BF16:
+        case TG_TEX_F16:
+            TG_REQUIRE(a.textures && aligned(a.textures, 8), TG_ERR_INVALID_ARG, "16-bit textures must be 8-byte aligned");
+            TG_REQUIRE(a.D == 3 || a.D == 4, TG_ERR_UNSUPPORTED, "16-bit textures support 3 or 4 channels");
+            break;
+        case TG_TEX_FP8_E4M3:
+            TG_REQUIRE(a.textures && aligned(a.textures, 4) && a.tex_scales, TG_ERR_INVALID_ARG,
+                       "FP8 textures need 4-byte alignment and per-Gaussian scales");
+            TG_REQUIRE(a.D == 3 || a.D == 4, TG_ERR_UNSUPPORTED, "FP8 textures support 3 or 4 channels");
+            break;
+        default: return fail(TG_ERR_UNSUPPORTED, "unknown texture format %d", a.tex_format);
+    }
+    if (a.tex_format != TG_TEX_NONE)
+        TG_REQUIRE(a.tex_rx >= 1 && a.tex_ry >= 1 && a.range_x > 0.f && a.range_y > 0.f, TG_ERR_INVALID_ARG,
+                   "bad texture size or range");
+    return TG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int tg_version(void) { return 1; }
+
+const char* tg_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t tg_kernel_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int tg_project_fwd(const tg_project_fwd_args* a, tg_stream_t stream) {
+    TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
+    TG_REQUIRE(a->C >= 0 && a->N >= 0, TG_ERR_INVALID_ARG, "negative sizes");
+    if ((int64_t)a->C * a->N == 0) return TG_OK;
+    TG_REQUIRE(a->means && a->quats && a->scales && a->viewmats && a->Ks && a->radii && a->means2d && a->depths &&
+                   a->ray_transforms && a->normals,
+               TG_ERR_INVALID_ARG, "null pointer");
+    TG_REQUIRE(aligned(a->quats, 16) && aligned(a->means2d, 8), TG_ERR_INVALID_ARG,
+               "quats must be 16-byte and means2d 8-byte aligned");
+    return cuda_status(tg::launch_project_fwd(*a, stream), "tg_project_fwd");
+}
+
+int tg_project_bwd(const tg_project_bwd_args* a, tg_stream_t stream) {
+    TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
+    TG_REQUIRE(a->C >= 0 && a->N >= 0, TG_ERR_INVALID_ARG, "negative sizes");
+    TG_REQUIRE(a->mode >= 0 && a->mode <= 2, TG_ERR_INVALID_ARG, "bad mode %d", a->mode);
+    if (a->N == 0) return TG_OK;
+    TG_REQUIRE(a->means && a->quats && a->scales && a->viewmats && a->Ks && a->radii && a->ray_transforms &&
+                   a->v_means2d && a->v_depths && a->v_normals && a->v_ray_transforms && a->v_means && a->v_quats &&
+                   a->v_scales,
+               TG_ERR_INVALID_ARG, "null pointer");
+    TG_REQUIRE(aligned(a->quats, 16) && aligned(a->v_quats, 16), TG_ERR_INVALID_ARG, "quats must be 16-byte aligned");
+    return cuda_status(tg::launch_project_bwd(*a, stream), "tg_project_bwd");
+}
+
+size_t tg_scan_workspace_bytes(int64_t n_elems) { return tg::scan_workspace_bytes(n_elems); }
+
+int tg_isect_count(const tg_isect_args* a, tg_stream_t stream) {
+    TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
+    TG_REQUIRE(a->n_elems >= 0 && a->n_elems < (int64_t(1) << 31), TG_ERR_INVALID_ARG, "n_elems out of range");
+    TG_REQUIRE(a->tile_size > 0 && a->tile_width > 0 && a->tile_height > 0 && a->n_cameras > 0, TG_ERR_INVALID_ARG,
+               "bad tile grid");
+    TG_REQUIRE(bit_width((int64_t)a->tile_width * a->tile_height) + bit_width(a->n_cameras) <= 32, TG_ERR_INVALID_ARG,
+               "camera and tile ids need more than 32 bits");
+    TG_REQUIRE(a->n_isects && a->scan_workspace, TG_ERR_INVALID_ARG, "null n_isects / workspace");
+    if (a->n_elems > 0)
+        TG_REQUIRE(a->means2d && a->radii && a->tiles_per_gauss && a->cum_tiles && aligned(a->means2d, 8),
+                   TG_ERR_INVALID_ARG, "null or misaligned pointer");
+    return cuda_status(tg::launch_isect_count(*a, stream), "tg_isect_count");
+}
+
+int tg_isect_emit(const tg_isect_args* a, tg_stream_t stream) {
+    TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
+    if (a->n_elems == 0) return TG_OK;
+    TG_REQUIRE(a->means2d && a->radii && a->depths && a->cum_tiles && a->isect_ids && a->flatten_ids,
+               TG_ERR_INVALID_ARG, "null pointer");
+    TG_REQUIRE(a->camera_ids != nullptr || a->N > 0, TG_ERR_INVALID_ARG, "dense layout needs N > 0");
+    const int tb = bit_width((int64_t)a->tile_width * a->tile_height);
+    return cuda_status(tg::launch_isect_emit(*a, tb, stream), "tg_isect_emit");
+}
+
+size_t tg_sort_workspace_bytes(int64_t n, int32_t end_bit) { return tg::sort_workspace_bytes(n, end_bit); }
+
+int tg_sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, int64_t n, int32_t end_bit,
+                  void* workspace, size_t workspace_bytes, int32_t* result_in_alt, tg_stream_t stream) {
+    TG_REQUIRE(result_in_alt != nullptr, TG_ERR_INVALID_ARG, "null result_in_alt");
+    *result_in_alt = 0;
+    TG_REQUIRE(n >= 0 && n < (int64_t(1) << 30), TG_ERR_INVALID_ARG, "sort supports up to 2^30 pairs");
+    TG_REQUIRE(end_bit >= 0 && end_bit <= 64, TG_ERR_INVALID_ARG, "bad end_bit %d", end_bit);
+    if (n <= 1) return TG_OK;
+    TG_REQUIRE(keys && vals && keys_alt && vals_alt && workspace, TG_ERR_INVALID_ARG, "null pointer");
+    cudaError_t cerr;
+    const int rc = tg::sort_pairs(keys, vals, keys_alt, vals_alt, n, end_bit, workspace, workspace_bytes,
+                                  result_in_alt, stream, cerr);
+    if (rc == TG_ERR_CUDA) return cuda_status(cerr, "tg_sort_pairs");
+    if (rc == TG_ERR_WORKSPACE) return fail(rc, "workspace of %zu bytes is smaller than %zu", workspace_bytes,
+                                            tg::sort_workspace_bytes(n, end_bit));
+    if (rc != TG_OK) return fail(rc, "tg_sort_pairs: invalid argument");
+    return TG_OK;
+}
+
+int tg_isect_offset_encode(const int64_t* isect_ids, int64_t n_isects, int32_t n_cameras, int32_t tile_width,
+                           int32_t tile_height, int32_t* offsets, tg_stream_t stream) {
+    TG_REQUIRE(n_cameras > 0 && tile_width > 0 && tile_height > 0 && offsets, TG_ERR_INVALID_ARG, "bad arguments");
+    TG_REQUIRE(n_isects >= 0 && (n_isects == 0 || isect_ids), TG_ERR_INVALID_ARG, "null isect_ids");
+    const int tb = bit_width((int64_t)tile_width * tile_height);
+    const int cb = bit_width(n_cameras);
+    return cuda_status(tg::launch_offset_encode(isect_ids, n_isects, n_cameras, tile_width, tile_height, tb,
+                                                32 + tb + cb, offsets, stream),
+                       "tg_isect_offset_encode");
+}
+
+int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream) {
+    TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
+    int rc = check_raster_common(*a);
+    if (rc != TG_OK) return rc;
+    const int64_t pixels = (int64_t)a->C * a->height * a->width;
+    if (pixels > 0)
+        TG_REQUIRE(a->out_colors && a->out_alphas && a->out_normals && a->out_distort && a->out_median &&
+                       a->last_ids && a->median_ids,
+                   TG_ERR_INVALID_ARG, "null output");
+    TG_REQUIRE(a->n_contrib >= 0 && (a->n_contrib == 0 || (a->contrib_sum && a->contrib_count)), TG_ERR_INVALID_ARG,
+               "null contribution buffers");
+    cudaError_t e = cudaSuccess;
+    if (a->n_contrib > 0) {
+        e = cudaMemsetAsync(a->contrib_sum, 0, sizeof(float) * a->n_contrib, stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(a->contrib_count, 0, sizeof(float) * a->n_contrib, stream);
+        if (e != cudaSuccess) return cuda_status(e, "tg_rasterize_fwd memset");
+    }
+    return cuda_status(tg::launch_raster_fwd(*a, stream), "tg_rasterize_fwd");
+}
+
+int tg_rasterize_bwd(const tg_raster_bwd_args* a, tg_stream_t stream) {
+    TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
+    int rc = check_raster_common(a->f);
+    if (rc != TG_OK) return rc;
+    TG_REQUIRE(a->adjoint >= 0 && a->adjoint <= 2, TG_ERR_INVALID_ARG, "bad adjoint %d", a->adjoint);
+    TG_REQUIRE(a->n_elems >= 0, TG_ERR_INVALID_ARG, "negative n_elems");
+    TG_REQUIRE(a->render_colors && a->render_alphas && a->last_ids && a->median_ids && a->v_render_colors &&
+                   a->v_render_alphas && a->v_render_normals && a->v_render_distort && a->v_render_median,
+               TG_ERR_INVALID_ARG, "null forward output or upstream gradient");
+    TG_REQUIRE(a->v_means2d && a->v_ray_transforms && a->v_colors && a->v_opacities && a->v_normals && a->v_densify,
+               TG_ERR_INVALID_ARG, "null gradient output");
+    if (a->v_textures) TG_REQUIRE(aligned(a->v_textures, 16), TG_ERR_INVALID_ARG, "v_textures must be 16-byte aligned");
+    const int64_t E = a->n_elems;
+    const int D = a->f.D;
+    const size_t tex_bytes = a->f.tex_format == TG_TEX_NONE || a->v_textures == nullptr
+                                 ? 0
+                                 : sizeof(float) * 4 * (size_t)a->f.tex_ry * a->f.tex_rx * (size_t)a->f.n_contrib;
+    struct Z { void* p; size_t n; } zs[] = {
+        {a->v_means2d, sizeof(float) * 2 * E}, {a->v_ray_transforms, sizeof(float) * 9 * E},
+        {a->v_colors, sizeof(float) * D * E},  {a->v_opacities, sizeof(float) * E},
+        {a->v_normals, sizeof(float) * 3 * E}, {a->v_means2d_abs, a->v_means2d_abs ? sizeof(float) * 2 * E : 0},
+        {a->v_textures, tex_bytes},            {a->v_densify, sizeof(float) * 2 * E}};
+    for (const Z& z : zs)
+        if (z.p && z.n) {
+            cudaError_t e = cudaMemsetAsync(z.p, 0, z.n, stream);
+            if (e != cudaSuccess) return cuda_status(e, "tg_rasterize_bwd memset");
+        }
+    return cuda_status(tg::launch_raster_bwd(*a, stream), "tg_rasterize_bwd");
+}
+
+int tg_sh_fwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, const float* dirs, const float* coeffs,
+              const uint8_t* masks, float* colors, tg_stream_t stream) {
+    TG_REQUIRE(n >= 0 && degree >= 0 && degree <= 4 && (degree + 1) * (degree + 1) <= K, TG_ERR_INVALID_ARG,
+               "bad SH degree %d for %d bases", degree, K);
+    if (n == 0) return TG_OK;
+    TG_REQUIRE(coeff_rows > 0 && n % coeff_rows == 0, TG_ERR_INVALID_ARG, "coeff_rows must divide n");
+    TG_REQUIRE(dirs && coeffs && colors, TG_ERR_INVALID_ARG, "null pointer");
+    return cuda_status(tg::launch_sh_fwd(n, coeff_rows, degree, K, dirs, coeffs, masks, colors, stream), "tg_sh_fwd");
+}
+
+int tg_sh_bwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, const float* dirs, const float* coeffs,
+              const uint8_t* masks, const float* v_colors, float* v_coeffs, float* v_dirs, tg_stream_t stream) {
+    TG_REQUIRE(n >= 0 && degree >= 0 && degree <= 4 && (degree + 1) * (degree + 1) <= K, TG_ERR_INVALID_ARG,
+               "bad SH degree %d for %d bases", degree, K);
+    if (n == 0) return TG_OK;
+    TG_REQUIRE(coeff_rows > 0 && n % coeff_rows == 0, TG_ERR_INVALID_ARG, "coeff_rows must divide n");
+    TG_REQUIRE(dirs && coeffs && v_colors && v_coeffs, TG_ERR_INVALID_ARG, "null pointer");
+    return cuda_status(
+        tg::launch_sh_bwd(n, coeff_rows, degree, K, dirs, coeffs, masks, v_colors, v_coeffs, v_dirs, stream),
+        "tg_sh_bwd");
+}
+
+}  // extern "C"

@@ -1,0 +1,371 @@
+// Textured / plain 2DGS compositor, adjoint, for sm_100a.
+//
+// One CTA per (camera, tile), one thread per pixel, back-to-front over the
+// splats that can still matter to the tile (batches beyond every pixel's last
+// contributor are skipped).  Transmittance is recovered from the stored final
+// T and last-contributor index by division, as the reference does
+// (rasterize_to_pixels_textured_gaussians_2dgs_bwd.cu:160, :456-457); nothing
+// per splat is stored by the forward.
+//
+// Reductions, B200-first:
+//  * per-splat gradients (colour, normal, ray transform, means2d, opacity,
+//    |means2d|) are reduced across the warp by a reduce-scatter butterfly --
+//    31 shuffles leave lane k holding the warp total of value k -- instead of
+//    one 5-level shuffle tree per value; lanes then add into a per-batch
+//    shared-memory accumulator, and the CTA flushes each splat's values with
+//    one global atomic per value (8x fewer global atomics than per-warp);
+//  * per-texel gradients are RGBA float4 vector atomics, one per bilinear tap
+//    (4 per pixel-splat pair instead of the reference's up to 4*(D+1) scalar
+//    atomics).
+//
+// Adjoint forms: TG_ADJ_REFERENCE follows ..._bwd.cu:438-627; TG_ADJ_BWD2 adds
+// the reference's texture-UV term (..._bwd2.cu:612-676, du/ds = (R-1)/range);
+// TG_ADJ_EXACT adds the UV term with the true du/ds = (R-1)/(2 range).
+#include "raster_common.cuh"
+
+namespace tg {
+
+// reduce-scatter: on return vals[0] of lane l holds the warp sum of value l.
+__device__ __forceinline__ void warp_reduce_scatter32(float (&vals)[32], unsigned mask) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool upper = (lane & s) != 0;
+        const bool have = ((mask >> (lane ^ s)) & 1u) != 0;
+#pragma unroll
+        for (int i = 0; i < s; ++i) {
+            const float send = upper ? vals[i] : vals[i + s];
+            const float keep = upper ? vals[i + s] : vals[i];
+            const float recv = __shfl_xor_sync(mask, send, s);
+            vals[i] = keep + (have ? recv : 0.f);
+        }
+    }
+}
+
+template <int D>
+struct GradSlots {
+    static constexpr int kRgb = 0;
+    static constexpr int kNrm = D;
+    static constexpr int kM = D + 3;
+    static constexpr int kXY = D + 12;
+    static constexpr int kOpac = D + 14;
+    static constexpr int kAbs = D + 15;
+    static constexpr int kCount = D + 17;
+};
+
+template <int D, class Tex>
+__global__ void __launch_bounds__(256) raster_bwd_kernel(const tg_raster_bwd_args a, const float uv_scale) {
+    constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
+    using GS = GradSlots<D>;
+    constexpr int NV = GS::kCount;
+    const tg_raster_fwd_args& f = a.f;
+    extern __shared__ float4 smem4[];
+    const int bs = blockDim.x;
+    float4* s_xyo = smem4;
+    float4* s_m0 = s_xyo + bs;
+    float4* s_m1 = s_m0 + bs;
+    float4* s_m2 = s_m1 + bs;
+    float4* s_nrm = s_m2 + bs;
+    float* s_col = reinterpret_cast<float*>(s_nrm + bs);
+    int* s_row = reinterpret_cast<int*>(s_col + bs * D);
+    int* s_g = s_row + bs;
+    float* s_grad = reinterpret_cast<float*>(s_g + bs);  // [bs][NV]
+    __shared__ int s_max_bin;
+
+    const unsigned wmask = __activemask();
+    const TileCoord tc = tile_of_block(f.tile_width, f.tile_height);
+    const int tr = threadIdx.x, lane = tr & 31;
+    const int per_cam = f.tile_width * f.tile_height;
+    if (f.masks != nullptr && !f.masks[(int64_t)tc.c * per_cam + tc.tile]) return;
+
+    const int ts = f.tile_size;
+    const int i = tc.ty * ts + tr / ts;
+    const int j = tc.tx * ts + tr % ts;
+    const bool inside = i < f.height && j < f.width;
+    const int64_t pix = ((int64_t)tc.c * f.height + i) * f.width + j;
+    const int64_t toff = (int64_t)tc.c * per_cam + tc.tile;
+    const int32_t range_start = f.tile_offsets[toff];
+    const int32_t range_end = (tc.c == f.C - 1 && tc.tile == per_cam - 1) ? (int32_t)f.n_isects : f.tile_offsets[toff + 1];
+
+    for (int k = tr; k < bs * NV; k += bs) s_grad[k] = 0.f;
+    if (tr == 0) s_max_bin = -1;
+
+    const float px = (float)j + 0.5f, py = (float)i + 0.5f;
+    float T_final = 1.f, v_a = 0.f, v_dist = 0.f, v_med = 0.f, bg_dot = 0.f;
+    float v_c[D], buf[D];
+    float v_n[3] = {0.f, 0.f, 0.f}, buf_n[3] = {0.f, 0.f, 0.f};
+    int32_t bin_final = -1, median_idx = -1;
+    float acc_d_buf = 0.f, acc_d = 0.f, acc_w_buf = 0.f, acc_w = 0.f, dist_buf = 0.f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) { v_c[k] = 0.f; buf[k] = 0.f; }
+    if (inside) {
+        const float alpha_out = a.render_alphas[pix];
+        T_final = 1.f - alpha_out;
+        bin_final = a.last_ids[pix];
+        median_idx = a.median_ids[pix];
+#pragma unroll
+        for (int k = 0; k < D; ++k) v_c[k] = a.v_render_colors[pix * D + k];
+        v_a = a.v_render_alphas[pix];
+        v_n[0] = a.v_render_normals[pix * 3];
+        v_n[1] = a.v_render_normals[pix * 3 + 1];
+        v_n[2] = a.v_render_normals[pix * 3 + 2];
+        v_dist = a.v_render_distort[pix];
+        v_med = a.v_render_median[pix];
+        acc_d_buf = a.render_colors[pix * D + D - 1];
+        acc_d = acc_d_buf;
+        acc_w_buf = alpha_out;
+        acc_w = alpha_out;
+        if (f.backgrounds) {
+#pragma unroll
+            for (int k = 0; k < D; ++k) bg_dot += f.backgrounds[tc.c * D + k] * v_c[k];
+        }
+    }
+    float T = T_final;
+    // last contributor over the warp and over the CTA
+    const int32_t warp_bin_final = __reduce_max_sync(wmask, bin_final);  // uniform across the warp
+    __syncthreads();
+    if (lane == __ffs(wmask) - 1) atomicMax(&s_max_bin, warp_bin_final);
+    __syncthreads();
+    const int32_t block_max_bin = s_max_bin;
+    const int64_t tex_stride = (int64_t)f.tex_ry * f.tex_rx;
+
+    for (int32_t batch_end = range_end - 1; batch_end >= range_start; batch_end -= bs) {
+        if (batch_end - (bs - 1) > block_max_bin) continue;  // every splat here is past all last contributors
+        const int32_t batch_size = min(bs, batch_end + 1 - range_start);
+        __syncthreads();  // previous batch fully flushed before restaging
+        const int32_t idx_load = batch_end - tr;
+        if (idx_load >= range_start) {
+            const int32_t g = f.flatten_ids[idx_load];
+            const float2 xy = reinterpret_cast<const float2*>(f.means2d)[g];
+            const int32_t row = f.gaussian_ids ? (int32_t)f.gaussian_ids[g] : g % f.N;
+            const float scale = (Tex::kFormat == TG_TEX_FP8_E4M3) ? f.tex_scales[row] : 1.f;
+            s_xyo[tr] = make_float4(xy.x, xy.y, f.opacities[g], scale);
+            const float* m = f.ray_transforms + 9 * (int64_t)g;
+            s_m0[tr] = make_float4(m[0], m[1], m[2], 0.f);
+            s_m1[tr] = make_float4(m[3], m[4], m[5], 0.f);
+            s_m2[tr] = make_float4(m[6], m[7], m[8], 0.f);
+            const float* n = f.normals + 3 * (int64_t)g;
+            s_nrm[tr] = make_float4(n[0], n[1], n[2], 0.f);
+#pragma unroll
+            for (int k = 0; k < D; ++k) s_col[tr * D + k] = f.colors[(int64_t)g * D + k];
+            s_row[tr] = row;
+            s_g[tr] = g;
+        }
+        __syncthreads();
+        for (int t = max(0, batch_end - warp_bin_final); t < batch_size; ++t) {
+            const int32_t idx = batch_end - t;
+            bool valid = inside && idx <= bin_final;
+            PairEval e;
+            const float4 xyo = s_xyo[t];
+            const int row = s_row[t];
+            if (valid) {
+                eval_pair<Tex>(e, px, py, xyo, s_m0[t], s_m1[t], s_m2[t], f.textures, (int64_t)row * tex_stride,
+                               f.tex_rx, f.tex_ry, f.range_x, f.range_y, f.g_weight);
+                valid = e.valid;
+            }
+            if (!__any_sync(wmask, valid)) continue;
+            float vals[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) vals[k] = 0.f;
+            if (valid) {
+                const float opac = xyo.z;
+                const float* cp = s_col + t * D;
+                const float4 nn = s_nrm[t];
+                if (idx == median_idx) vals[GS::kRgb + D - 1] += v_med;
+                const float ra = 1.f / (1.f - e.alpha);
+                T *= ra;
+                const float fac = e.alpha * T;
+                float texc[D];
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    vals[GS::kRgb + k] += fac * v_c[k];
+                    texc[k] = kTextured ? tex_color(e, k) : 0.f;
+                }
+                float v_alpha = 0.f;
+#pragma unroll
+                for (int k = 0; k < D; ++k) v_alpha += ((texc[k] + cp[k]) * T - buf[k] * ra) * v_c[k];
+                vals[GS::kNrm + 0] = fac * v_n[0];
+                vals[GS::kNrm + 1] = fac * v_n[1];
+                vals[GS::kNrm + 2] = fac * v_n[2];
+                v_alpha += (nn.x * T - buf_n[0] * ra) * v_n[0];
+                v_alpha += (nn.y * T - buf_n[1] * ra) * v_n[1];
+                v_alpha += (nn.z * T - buf_n[2] * ra) * v_n[2];
+                v_alpha += T_final * ra * v_a;
+                if (f.backgrounds) v_alpha += -T_final * ra * bg_dot;
+                {
+                    const float depth = cp[D - 1];
+                    const float dl_dw = 2.f * (2.f * (depth * acc_w_buf - acc_d_buf) + (acc_d - depth * acc_w));
+                    v_alpha += (dl_dw * T - dist_buf * ra) * v_dist;
+                    acc_d_buf -= fac * depth;
+                    acc_w_buf -= fac;
+                    dist_buf += dl_dw * fac;
+                    vals[GS::kRgb + D - 1] += 2.f * fac * (2.f - 2.f * T - acc_w + fac) * v_dist;
+                }
+                f3 vM0 = mk3(0, 0, 0), vM1 = mk3(0, 0, 0), vM2 = mk3(0, 0, 0);
+                const bool unclamped = kTextured ? (opac * e.vis * e.asf <= 0.999f) : (opac * e.vis <= 0.999f);
+                float tex_a_grad = 0.f;  // d L / d (texture alpha) / w_i
+                if (unclamped) {
+                    const float v_G = kTextured ? opac * v_alpha * e.asf : opac * v_alpha;
+                    const float dG = kTextured ? -f.g_weight * e.kern : -e.vis;
+                    if (e.g3 <= e.g2) {
+                        const float vsx = v_G * dG * e.sx, vsy = v_G * dG * e.sy;
+                        const float a_ = vsx / e.z.z, b_ = vsy / e.z.z;
+                        const f3 vz = mk3(a_, b_, -(a_ * e.sx + b_ * e.sy));
+                        const f3 vhu = cross(e.hv, vz), vhv = cross(vz, e.hu);
+                        vM0 = -1.f * vhu;
+                        vM1 = -1.f * vhv;
+                        vM2 = px * vhu + py * vhv;
+                    } else {
+                        const float vx = v_G * (dG * kFilterInvSquare * e.dx);
+                        const float vy = v_G * (dG * kFilterInvSquare * e.dy);
+                        vals[GS::kXY] = vx;
+                        vals[GS::kXY + 1] = vy;
+                        vals[GS::kAbs] = fabsf(vx);
+                        vals[GS::kAbs + 1] = fabsf(vy);
+                    }
+                    vals[GS::kOpac] = kTextured ? e.vis * v_alpha * e.asf : e.vis * v_alpha;
+                    tex_a_grad = e.vis * opac * v_alpha;
+                }
+                if (kTextured && e.tex_valid && a.v_textures != nullptr) {
+                    float* vt = a.v_textures + 4 * ((int64_t)row * tex_stride);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float4 gq;
+                        gq.x = 0 < D ? fac * e.w[q] * v_c[0] : 0.f;
+                        gq.y = 1 < D ? fac * e.w[q] * v_c[1 < D ? 1 : 0] : 0.f;
+                        gq.z = 2 < D ? fac * e.w[q] * v_c[2 < D ? 2 : 0] : 0.f;
+                        gq.w = (3 < D ? fac * e.w[q] * v_c[3 < D ? 3 : 0] : 0.f) + e.w[q] * tex_a_grad;
+                        if (gq.x != 0.f || gq.y != 0.f || gq.z != 0.f || gq.w != 0.f)
+                            atomicAdd(reinterpret_cast<float4*>(vt + 4 * (int64_t)e.toff[q]), gq);
+                    }
+                    if (uv_scale != 0.f) {
+                        const float wu = e.w[1] + e.w[3], wv = e.w[2] + e.w[3];
+                        const float dbu[4] = {-(1.f - wv), 1.f - wv, -wv, wv};
+                        const float dbv[4] = {-(1.f - wu), -wu, 1.f - wu, wu};
+                        const float du = uv_scale * (float)(f.tex_rx - 1) / f.range_x;
+                        const float dv = uv_scale * (float)(f.tex_ry - 1) / f.range_y;
+                        float tsx = 0.f, tsy = 0.f;
+#pragma unroll
+                        for (int k = 0; k < D && k < 4; ++k) {
+                            const float vt_k = fac * v_c[k];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                const float tv = f4get(e.tx[q], k);
+                                tsx += vt_k * dbu[q] * tv * du;
+                                tsy += vt_k * dbv[q] * tv * dv;
+                            }
+                        }
+                        if (unclamped) {
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                tsx += tex_a_grad * dbu[q] * e.tx[q].w * du;
+                                tsy += tex_a_grad * dbv[q] * e.tx[q].w * dv;
+                            }
+                        }
+                        const float a_ = tsx / e.z.z, b_ = tsy / e.z.z;
+                        const f3 vz = mk3(a_, b_, -(a_ * e.sx + b_ * e.sy));
+                        const f3 vhu = cross(e.hv, vz), vhv = cross(vz, e.hu);
+                        vM0 = vM0 - vhu;
+                        vM1 = vM1 - vhv;
+                        vM2 = vM2 + (px * vhu + py * vhv);
+                    }
+                }
+                vals[GS::kM + 0] = vM0.x; vals[GS::kM + 1] = vM0.y; vals[GS::kM + 2] = vM0.z;
+                vals[GS::kM + 3] = vM1.x; vals[GS::kM + 4] = vM1.y; vals[GS::kM + 5] = vM1.z;
+                vals[GS::kM + 6] = vM2.x; vals[GS::kM + 7] = vM2.y; vals[GS::kM + 8] = vM2.z;
+#pragma unroll
+                for (int k = 0; k < D; ++k) buf[k] += (texc[k] + cp[k]) * fac;
+                buf_n[0] += nn.x * fac;
+                buf_n[1] += nn.y * fac;
+                buf_n[2] += nn.z * fac;
+            }
+            warp_reduce_scatter32(vals, wmask);
+            if (lane < NV && vals[0] != 0.f) atomicAdd(s_grad + t * NV + lane, vals[0]);
+        }
+        __syncthreads();
+        // flush this batch's per-splat sums: one global atomic per (splat, value)
+        for (int k = tr; k < batch_size * NV; k += bs) {
+            const float v = s_grad[k];
+            if (v == 0.f) continue;
+            s_grad[k] = 0.f;
+            const int t = k / NV, slot = k - t * NV;
+            const int64_t g = s_g[t];
+            float* dst;
+            if (slot < GS::kNrm) dst = a.v_colors + g * D + slot;
+            else if (slot < GS::kM) dst = a.v_normals + g * 3 + (slot - GS::kNrm);
+            else if (slot < GS::kXY) dst = a.v_ray_transforms + g * 9 + (slot - GS::kM);
+            else if (slot < GS::kOpac) dst = a.v_means2d + g * 2 + (slot - GS::kXY);
+            else if (slot == GS::kOpac) dst = a.v_opacities + g;
+            else dst = a.v_means2d_abs ? a.v_means2d_abs + g * 2 + (slot - GS::kAbs) : nullptr;
+            if (dst) atomicAdd(dst, v);
+        }
+    }
+}
+
+// v_densify[e] = (v_M[e][2], v_M[e][5]) * M[e][8], once every contribution is in.
+__global__ void densify_grad_kernel(const float* __restrict__ v_M, const float* __restrict__ M, int64_t n,
+                                    float* __restrict__ v_densify) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const float depth = M[9 * e + 8];
+    v_densify[2 * e] = v_M[9 * e + 2] * depth;
+    v_densify[2 * e + 1] = v_M[9 * e + 5] * depth;
+}
+
+template <int D, class Tex>
+cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
+    const tg_raster_fwd_args& f = a.f;
+    const int bs = f.tile_size * f.tile_size;
+    const size_t smem = (size_t)bs * (5 * sizeof(float4) + D * sizeof(float) + 2 * sizeof(int) +
+                                      GradSlots<D>::kCount * sizeof(float));
+    const int64_t blocks = (int64_t)f.C * f.tile_width * f.tile_height;
+    const float uv_scale = a.adjoint == TG_ADJ_BWD2 ? 1.f : (a.adjoint == TG_ADJ_EXACT ? 0.5f : 0.f);
+    cudaError_t err = cudaFuncSetAttribute(raster_bwd_kernel<D, Tex>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+    if (err != cudaSuccess) return err;
+    if (blocks > 0 && f.n_isects > 0) {
+        raster_bwd_kernel<D, Tex><<<(unsigned)blocks, bs, smem, s>>>(a, uv_scale);
+        note_launches(1);
+    }
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    if (a.n_elems > 0)
+        densify_grad_kernel<<<(unsigned)((a.n_elems + 255) / 256), 256, 0, s>>>(a.v_ray_transforms,
+                                                                               f.ray_transforms, a.n_elems,
+                                                                               a.v_densify);
+    if (a.n_elems > 0) note_launches(1);
+    return cudaGetLastError();
+}
+
+template <class Tex>
+cudaError_t launch_bwd_d(const tg_raster_bwd_args& a, cudaStream_t s) {
+    switch (a.f.D) {
+        case 1: return launch_bwd_t<1, Tex>(a, s);
+        case 2: return launch_bwd_t<2, Tex>(a, s);
+        case 3: return launch_bwd_t<3, Tex>(a, s);
+        case 4: return launch_bwd_t<4, Tex>(a, s);
+        case 5: return launch_bwd_t<5, Tex>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <class Tex>
+cudaError_t launch_bwd_d34(const tg_raster_bwd_args& a, cudaStream_t s) {
+    switch (a.f.D) {
+        case 3: return launch_bwd_t<3, Tex>(a, s);
+        case 4: return launch_bwd_t<4, Tex>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_raster_bwd(const tg_raster_bwd_args& a, cudaStream_t s) {
+    switch (a.f.tex_format) {
+        case TG_TEX_NONE: return launch_bwd_d<TexNone>(a, s);
+        case TG_TEX_F32: return launch_bwd_d<TexF32>(a, s);
+        case TG_TEX_BF16: return launch_bwd_d34<TexBF16>(a, s);
+        case TG_TEX_F16: return launch_bwd_d34<TexF16>(a, s);
+        case TG_TEX_FP8_E4M3: return launch_bwd_d34<TexFP8>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace tg

@@ -1,0 +1,24 @@
+"""Op surface mirroring textured_gaussians.cuda (see _wrapper.py)."""
+from ._wrapper import (
+    fully_fused_projection_2dgs,
+    isect_offset_encode,
+    isect_tiles,
+    make_texture_storage,
+    rasterize_to_pixels_2dgs,
+    rasterize_to_pixels_textured_gaussians,
+    sort_pairs,
+    spherical_harmonics,
+    spherical_harmonics_shared,
+)
+
+__all__ = [
+    "fully_fused_projection_2dgs",
+    "isect_offset_encode",
+    "isect_tiles",
+    "make_texture_storage",
+    "rasterize_to_pixels_2dgs",
+    "rasterize_to_pixels_textured_gaussians",
+    "sort_pairs",
+    "spherical_harmonics",
+    "spherical_harmonics_shared",
+]

@@ -1,0 +1,593 @@
+"""Drop-in op surface of the textured 2DGS path, backed by libtg2dgs.so.
+
+Names, signatures, return tuples, dtypes and layouts follow the reference's
+``textured_gaussians/cuda/_wrapper.py``:
+
+=================================================  ====================================
+this module                                        reference (textured_gaussians/...)
+=================================================  ====================================
+``spherical_harmonics``                            cuda/_wrapper.py:54-80, 1233-1263
+``fully_fused_projection_2dgs``                    cuda/_wrapper.py:1267-1371, 1374-1484
+``isect_tiles``                                    cuda/_wrapper.py:349-420
+``isect_offset_encode``                            cuda/_wrapper.py:423-440
+``rasterize_to_pixels_2dgs``                       cuda/_wrapper.py:1647-1784, 2767-2944
+``rasterize_to_pixels_textured_gaussians``         cuda/_wrapper.py:1806-2002, 2947-3155
+=================================================  ====================================
+
+Every op runs hand-written sm_100a kernels through the C ABI; none has a CPU
+path.  Additions beyond the reference are keyword-only and default off:
+``filtering="bilinear_exact"`` (exact adjoint), ``texture_storage`` /
+``texture_scales`` (BF16 / FP16 / FP8-E4M3 texture sampling with FP32
+gradients), and ``adjoint="exact"`` on the projection.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Optional, Tuple
+
+import torch
+from torch import Tensor
+
+from .. import _backend as B
+
+_FILTER_ADJOINT = {
+    "bilinear": B.TG_ADJ_REFERENCE,
+    "bilinear_bwd2": B.TG_ADJ_BWD2,
+    "bilinear_exact": B.TG_ADJ_EXACT,
+}
+
+
+def _bit_width(n: int) -> int:
+    return int(n).bit_length()
+
+
+# --------------------------------------------------------------------------- SH
+def spherical_harmonics(degrees_to_use: int, dirs: Tensor, coeffs: Tensor, masks: Optional[Tensor] = None) -> Tensor:
+    """Computes spherical harmonics (reference: cuda/_wrapper.py:54-80).
+
+    Args:
+        degrees_to_use: The degree to be used.
+        dirs: Directions. [..., 3]
+        coeffs: Coefficients. [..., K, 3]
+        masks: Optional boolean masks to skip some computation. [...,]
+
+    Returns:
+        Spherical harmonics. [..., 3]
+    """
+    assert (degrees_to_use + 1) ** 2 <= coeffs.shape[-2], coeffs.shape
+    assert dirs.shape[:-1] == coeffs.shape[:-2], (dirs.shape, coeffs.shape)
+    assert dirs.shape[-1] == 3, dirs.shape
+    assert coeffs.shape[-1] == 3, coeffs.shape
+    if masks is not None:
+        assert masks.shape == dirs.shape[:-1], masks.shape
+        masks = masks.contiguous()
+    return _SphericalHarmonics.apply(degrees_to_use, dirs.contiguous(), coeffs.contiguous(), masks, 1)
+
+
+def spherical_harmonics_shared(degrees_to_use: int, dirs: Tensor, coeffs: Tensor,
+                               masks: Optional[Tensor] = None) -> Tensor:
+    """SH colours for C cameras sharing one coefficient table.
+
+    dirs [C, N, 3], coeffs [N, K, 3] -> colours [C, N, 3]; the same values as
+    ``spherical_harmonics(d, dirs, coeffs.expand(C, ...), masks)`` without
+    materialising C copies of the coefficients.
+    """
+    C = dirs.shape[0]
+    assert dirs.dim() == 3 and coeffs.dim() == 3 and dirs.shape[1] == coeffs.shape[0], (dirs.shape, coeffs.shape)
+    assert (degrees_to_use + 1) ** 2 <= coeffs.shape[-2], coeffs.shape
+    if masks is not None:
+        masks = masks.contiguous()
+    return _SphericalHarmonics.apply(degrees_to_use, dirs.contiguous(), coeffs.contiguous(), masks, C)
+
+
+class _SphericalHarmonics(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, sh_degree: int, dirs: Tensor, coeffs: Tensor, masks: Optional[Tensor], share: int) -> Tensor:
+        dirs_f = dirs.float().contiguous()
+        coeffs_f = coeffs.float().contiguous()
+        n = dirs_f.numel() // 3
+        K = coeffs_f.shape[-2]
+        rows = coeffs_f.numel() // (3 * K) if coeffs_f.numel() else 0
+        colors = torch.empty(dirs_f.shape, dtype=torch.float32, device=dirs.device)
+        m = None if masks is None else masks.to(torch.uint8).contiguous()
+        if n:
+            st = B.stream_of(dirs)
+            B.call("tg_sh_fwd", st, B.lib().tg_sh_fwd, n, rows, sh_degree, K, B.ptr(dirs_f), B.ptr(coeffs_f), B.ptr(m),
+                   B.ptr(colors), st)
+        ctx.save_for_backward(dirs_f, coeffs_f, m)
+        ctx.sh_degree = sh_degree
+        ctx.share = share
+        return colors
+
+    @staticmethod
+    def backward(ctx, v_colors: Tensor):
+        dirs, coeffs, m = ctx.saved_tensors
+        n = dirs.numel() // 3
+        K = coeffs.shape[-2]
+        rows = coeffs.numel() // (3 * K) if coeffs.numel() else 0
+        compute_v_dirs = ctx.needs_input_grad[1]
+        v_coeffs = torch.empty_like(coeffs)
+        v_dirs = torch.empty_like(dirs) if compute_v_dirs else None
+        vc = v_colors.float().contiguous()
+        if n:
+            st = B.stream_of(dirs)
+            B.call("tg_sh_bwd", st, B.lib().tg_sh_bwd, n, rows, ctx.sh_degree, K, B.ptr(dirs), B.ptr(coeffs), B.ptr(m),
+                   B.ptr(vc), B.ptr(v_coeffs), B.ptr(v_dirs), st)
+        else:
+            v_coeffs.zero_()
+        return None, v_dirs, v_coeffs, None, None
+
+
+# --------------------------------------------------------------------------- projection
+def fully_fused_projection_2dgs(
+    means: Tensor,
+    quats: Tensor,
+    scales: Tensor,
+    viewmats: Tensor,
+    Ks: Tensor,
+    width: int,
+    height: int,
+    eps2d: float = 0.3,
+    near_plane: float = 0.01,
+    far_plane: float = 1e10,
+    radius_clip: float = 0.0,
+    packed: bool = False,
+    sparse_grad: bool = False,
+    norm_rot_grad: bool = False,
+    *,
+    adjoint: str = "reference",
+) -> Tuple[Tensor, ...]:
+    """Ray-splat transforms, 2D means, depths, screen radii and normals
+    (reference: cuda/_wrapper.py:1267-1371).
+
+    Returns ``(radii, means2d, depths, ray_transforms, normals)`` for the dense
+    layout.  ``adjoint="exact"`` selects the exact derivative of means2d with
+    respect to the ray transform in the backward (the reference keeps only its
+    diagonal terms).
+    """
+    C = viewmats.size(0)
+    N = means.size(0)
+    assert means.size() == (N, 3), means.size()
+    assert viewmats.size() == (C, 4, 4), viewmats.size()
+    assert Ks.size() == (C, 3, 3), Ks.size()
+    assert quats is not None, "quats is required"
+    assert scales is not None, "scales is required"
+    assert quats.size() == (N, 4), quats.size()
+    assert scales.size() == (N, 3), scales.size()
+    if sparse_grad:
+        assert packed, "sparse_grad is only supported when packed is True"
+    if packed:
+        raise NotImplementedError("packed=True projection is not available in this build")
+    mode = B.TG_ADJ_EXACT if adjoint == "exact" else (B.TG_ADJ_BWD2 if norm_rot_grad else B.TG_ADJ_REFERENCE)
+    return _FullyFusedProjection2DGS.apply(
+        means.contiguous(), quats.contiguous(), scales.contiguous(), viewmats.contiguous(), Ks.contiguous(),
+        width, height, eps2d, near_plane, far_plane, radius_clip, mode)
+
+
+class _FullyFusedProjection2DGS(torch.autograd.Function):
+    """Projects Gaussians to 2D (reference: cuda/_wrapper.py:1374-1484)."""
+
+    @staticmethod
+    def forward(ctx, means, quats, scales, viewmats, Ks, width, height, eps2d, near_plane, far_plane, radius_clip,
+                mode):
+        C, N = viewmats.shape[0], means.shape[0]
+        dev = means.device
+        radii = torch.empty((C, N), dtype=torch.int32, device=dev)
+        means2d = torch.empty((C, N, 2), dtype=torch.float32, device=dev)
+        depths = torch.empty((C, N), dtype=torch.float32, device=dev)
+        ray_transforms = torch.empty((C, N, 3, 3), dtype=torch.float32, device=dev)
+        normals = torch.empty((C, N, 3), dtype=torch.float32, device=dev)
+        a = B.ProjectFwdArgs(C, N, B.ptr(means), B.ptr(quats), B.ptr(scales), B.ptr(viewmats), B.ptr(Ks),
+                             int(width), int(height), float(near_plane), float(far_plane), float(radius_clip),
+                             B.ptr(radii), B.ptr(means2d), B.ptr(depths), B.ptr(ray_transforms), B.ptr(normals))
+        if C * N:
+            st = B.stream_of(means)
+            B.call("tg_project_fwd", st, B.lib().tg_project_fwd, ctypes.byref(a), st)
+        ctx.save_for_backward(means, quats, scales, viewmats, Ks, radii, ray_transforms)
+        ctx.mode = mode
+        ctx.mark_non_differentiable(radii)
+        return radii, means2d, depths, ray_transforms, normals
+
+    @staticmethod
+    def backward(ctx, v_radii, v_means2d, v_depths, v_ray_transforms, v_normals):
+        means, quats, scales, viewmats, Ks, radii, ray_transforms = ctx.saved_tensors
+        C, N = viewmats.shape[0], means.shape[0]
+
+        def z(t, shape):
+            return torch.zeros(shape, dtype=torch.float32, device=means.device) if t is None else t.float().contiguous()
+
+        v_means2d = z(v_means2d, (C, N, 2))
+        v_depths = z(v_depths, (C, N))
+        v_ray_transforms = z(v_ray_transforms, (C, N, 3, 3))
+        v_normals = z(v_normals, (C, N, 3))
+        v_means = torch.empty_like(means)
+        v_quats = torch.empty_like(quats)
+        v_scales = torch.empty_like(scales)
+        a = B.ProjectBwdArgs(C, N, B.ptr(means), B.ptr(quats), B.ptr(scales), B.ptr(viewmats), B.ptr(Ks),
+                             B.ptr(radii), B.ptr(ray_transforms), B.ptr(v_means2d), B.ptr(v_depths),
+                             B.ptr(v_normals), B.ptr(v_ray_transforms), ctx.mode, B.ptr(v_means), B.ptr(v_quats),
+                             B.ptr(v_scales))
+        if N:
+            st = B.stream_of(means)
+            B.call("tg_project_bwd", st, B.lib().tg_project_bwd, ctypes.byref(a), st)
+        v_viewmats = torch.zeros_like(viewmats) if ctx.needs_input_grad[3] else None  # never written (reference)
+        return (v_means if ctx.needs_input_grad[0] else None, v_quats if ctx.needs_input_grad[1] else None,
+                v_scales if ctx.needs_input_grad[2] else None, v_viewmats,
+                None, None, None, None, None, None, None, None)
+
+
+# --------------------------------------------------------------------------- intersection
+@torch.no_grad()
+def isect_tiles(
+    means2d: Tensor,
+    radii: Tensor,
+    depths: Tensor,
+    tile_size: int,
+    tile_width: int,
+    tile_height: int,
+    sort: bool = True,
+    packed: bool = False,
+    n_cameras: Optional[int] = None,
+    camera_ids: Optional[Tensor] = None,
+    gaussian_ids: Optional[Tensor] = None,
+) -> Tuple[Tensor, Tensor, Tensor]:
+    """Maps projected Gaussians to intersecting tiles (reference: cuda/_wrapper.py:349-420).
+
+    Returns ``(tiles_per_gauss int32 [C,N] or [nnz], isect_ids int64 [n_isects],
+    flatten_ids int32 [n_isects])``, sorted stably by isect id when ``sort``.
+    """
+    if packed:
+        nnz = means2d.size(0)
+        assert means2d.shape == (nnz, 2), means2d.size()
+        assert radii.shape == (nnz,), radii.size()
+        assert depths.shape == (nnz,), depths.size()
+        assert camera_ids is not None, "camera_ids is required if packed is True"
+        assert gaussian_ids is not None, "gaussian_ids is required if packed is True"
+        assert n_cameras is not None, "n_cameras is required if packed is True"
+        C, N, E = n_cameras, 0, nnz
+        cam = camera_ids.contiguous().long()
+    else:
+        C, N, _ = means2d.shape
+        assert means2d.shape == (C, N, 2), means2d.size()
+        assert radii.shape == (C, N), radii.size()
+        assert depths.shape == (C, N), depths.size()
+        E = C * N
+        cam = None
+    dev = means2d.device
+    means2d = means2d.float().contiguous()
+    radii = radii.int().contiguous()
+    depths = depths.float().contiguous()
+    tiles_per_gauss = torch.empty(radii.shape, dtype=torch.int32, device=dev)
+    cum = torch.empty((max(E, 1),), dtype=torch.int64, device=dev)
+    n_dev = torch.empty((1,), dtype=torch.int64, device=dev)
+    ws = torch.empty((B.lib().tg_scan_workspace_bytes(E),), dtype=torch.uint8, device=dev)
+    a = B.IsectArgs(E, N, B.ptr(cam), B.ptr(means2d), B.ptr(radii), B.ptr(depths), int(tile_size), int(tile_width),
+                    int(tile_height), int(C), B.ptr(tiles_per_gauss), B.ptr(cum), B.ptr(n_dev), B.ptr(ws), None, None)
+    stream = B.stream_of(means2d)
+    B.call("tg_isect_count", stream, B.lib().tg_isect_count, ctypes.byref(a), stream)
+    n_isects = int(n_dev.item())  # the one host synchronisation, as in the reference
+    isect_ids = torch.empty((n_isects,), dtype=torch.int64, device=dev)
+    flatten_ids = torch.empty((n_isects,), dtype=torch.int32, device=dev)
+    if n_isects:
+        a.isect_ids = B.ptr(isect_ids)
+        a.flatten_ids = B.ptr(flatten_ids)
+        B.call("tg_isect_emit", stream, B.lib().tg_isect_emit, ctypes.byref(a), stream)
+        if sort:
+            end_bit = 32 + _bit_width(tile_width * tile_height) + _bit_width(C)
+            isect_ids, flatten_ids = sort_pairs(isect_ids, flatten_ids, end_bit)
+    return tiles_per_gauss, isect_ids, flatten_ids
+
+
+def sort_pairs(keys: Tensor, vals: Tensor, end_bit: int) -> Tuple[Tensor, Tensor]:
+    """Stable radix sort of (int64 key, int32 value) pairs on key bits [0, end_bit)."""
+    n = keys.numel()
+    if n <= 1:
+        return keys, vals
+    keys_alt = torch.empty_like(keys)
+    vals_alt = torch.empty_like(vals)
+    wsb = B.lib().tg_sort_workspace_bytes(n, end_bit)
+    ws = torch.empty((wsb,), dtype=torch.uint8, device=keys.device)
+    in_alt = ctypes.c_int32(0)
+    st = B.stream_of(keys)
+    B.call("tg_sort_pairs", st, B.lib().tg_sort_pairs, B.ptr(keys), B.ptr(vals), B.ptr(keys_alt), B.ptr(vals_alt), n,
+           end_bit, B.ptr(ws), wsb, ctypes.byref(in_alt), st)
+    return (keys_alt, vals_alt) if in_alt.value else (keys, vals)
+
+
+@torch.no_grad()
+def isect_offset_encode(isect_ids: Tensor, n_cameras: int, tile_width: int, tile_height: int) -> Tensor:
+    """Encodes intersection ids to offsets (reference: cuda/_wrapper.py:423-440). [C, tile_height, tile_width]"""
+    isect_ids = isect_ids.contiguous()
+    offsets = torch.empty((n_cameras, tile_height, tile_width), dtype=torch.int32, device=isect_ids.device)
+    st = B.stream_of(isect_ids)
+    B.call("tg_isect_offset_encode", st, B.lib().tg_isect_offset_encode, B.ptr(isect_ids), isect_ids.numel(),
+           int(n_cameras), int(tile_width), int(tile_height), B.ptr(offsets), st)
+    return offsets
+
+
+# --------------------------------------------------------------------------- compositor
+_SUPPORTED_PADDED = (1, 2, 3, 4, 8, 16, 32, 64, 128, 256, 512)
+
+
+def _pad_channels(colors: Tensor, backgrounds: Optional[Tensor]):
+    """Channel padding rule of the reference (cuda/_wrapper.py:1880-1899)."""
+    channels = colors.shape[-1]
+    if channels > 512 or channels == 0:
+        raise ValueError(f"Unsupported number of color channels: {channels}")
+    if channels not in _SUPPORTED_PADDED:
+        padded = (1 << (channels - 1).bit_length()) - channels
+        colors = torch.cat([colors, torch.zeros(*colors.shape[:-1], padded, device=colors.device)], dim=-1)
+        if backgrounds is not None:
+            backgrounds = torch.cat(
+                [backgrounds, torch.zeros(*backgrounds.shape[:-1], padded, device=backgrounds.device)], dim=-1)
+    else:
+        padded = 0
+    return colors, backgrounds, padded
+
+
+def _tex_format(storage: Tensor) -> int:
+    if storage.dtype == torch.float32:
+        return B.TG_TEX_F32
+    if storage.dtype == torch.bfloat16:
+        return B.TG_TEX_BF16
+    if storage.dtype == torch.float16:
+        return B.TG_TEX_F16
+    if storage.dtype == torch.float8_e4m3fn:
+        return B.TG_TEX_FP8_E4M3
+    raise TypeError(f"unsupported texture dtype {storage.dtype}")
+
+
+def make_texture_storage(textures: Tensor, fmt: str) -> Tuple[Tensor, Optional[Tensor]]:
+    """Low-precision copy of FP32 textures for sampling: "bf16", "fp16" or "fp8".
+
+    FP8-E4M3 uses one scale per Gaussian, max|texel| / 448, returned as the
+    second element (None for the 16-bit forms).
+    """
+    if fmt == "bf16":
+        return textures.to(torch.bfloat16).contiguous(), None
+    if fmt == "fp16":
+        return textures.to(torch.float16).contiguous(), None
+    if fmt == "fp8":
+        amax = textures.detach().abs().flatten(1).amax(dim=1).clamp_min(1e-12)
+        scales = (amax / 448.0).float().contiguous()
+        q = (textures.detach() / scales[:, None, None, None]).to(torch.float8_e4m3fn).contiguous()
+        return q, scales
+    if fmt == "fp32":
+        return textures.float().contiguous(), None
+    raise ValueError(f"unknown texture storage format {fmt!r}")
+
+
+def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_store, tex_scales, range_x, range_y,
+              backgrounds, masks, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
+              gs_contrib_threshold, g_weight, C, N):
+    D = colors.shape[-1]
+    th, tw = isect_offsets.shape[1:3]
+    if textures_store is None:
+        fmt, ry, rx = B.TG_TEX_NONE, 0, 0
+    else:
+        fmt, ry, rx = _tex_format(textures_store), textures_store.shape[1], textures_store.shape[2]
+    return B.RasterFwdArgs(
+        C, N, D, int(width), int(height), int(tile_size), int(tw), int(th), flatten_ids.numel(), B.ptr(means2d),
+        B.ptr(ray_transforms), B.ptr(colors), B.ptr(opacities), B.ptr(normals), fmt, B.ptr(textures_store),
+        B.ptr(tex_scales), ry, rx, float(range_x), float(range_y), B.ptr(backgrounds), B.ptr(masks),
+        B.ptr(isect_offsets), B.ptr(flatten_ids), B.ptr(gaussian_ids), float(gs_contrib_threshold), float(g_weight),
+        int(n_contrib), None, None, None, None, None, None, None, None, None)
+
+
+class _RasterizeToPixelsTextured(torch.autograd.Function):
+    """Compositor forward/adjoint for both the textured and the plain form.
+
+    Mirrors _RasterizeToPixelsTexturedGaussians (reference cuda/_wrapper.py:2947-3155)
+    and _RasterizeToPixels2DGS (:2767-2944): saves the inputs plus the final
+    colours, alphas, last and median ids -- no per-splat transmittance.
+    """
+
+    @staticmethod
+    def forward(ctx, means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, masks,
+                tex_store, tex_scales, range_x, range_y, width, height, tile_size, isect_offsets, flatten_ids,
+                absgrad, gs_contrib_threshold, g_weight, adjoint, bg_grad_index_ok):
+        dev = means2d.device
+        packed = means2d.dim() == 2
+        C = isect_offsets.shape[0]
+        if packed:
+            raise NotImplementedError("packed rasterization is not available in this build")
+        N = means2d.shape[1]
+        n_contrib = N
+        D = colors.shape[-1]
+        m = None if masks is None else masks.to(torch.uint8).contiguous()
+        a = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
+                      backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, None, n_contrib,
+                      gs_contrib_threshold, g_weight, C, N)
+        render_colors = torch.empty((C, height, width, D), dtype=torch.float32, device=dev)
+        render_alphas = torch.empty((C, height, width, 1), dtype=torch.float32, device=dev)
+        render_normals = torch.empty((C, height, width, 3), dtype=torch.float32, device=dev)
+        render_distort = torch.empty((C, height, width, 1), dtype=torch.float32, device=dev)
+        render_median = torch.empty((C, height, width, 1), dtype=torch.float32, device=dev)
+        last_ids = torch.empty((C, height, width), dtype=torch.int32, device=dev)
+        median_ids = torch.empty((C, height, width), dtype=torch.int32, device=dev)
+        contrib_sum = torch.empty((n_contrib,), dtype=torch.float32, device=dev)
+        contrib_count = torch.empty((n_contrib,), dtype=torch.float32, device=dev)
+        a.out_colors, a.out_alphas, a.out_normals = B.ptr(render_colors), B.ptr(render_alphas), B.ptr(render_normals)
+        a.out_distort, a.out_median = B.ptr(render_distort), B.ptr(render_median)
+        a.last_ids, a.median_ids = B.ptr(last_ids), B.ptr(median_ids)
+        a.contrib_sum, a.contrib_count = B.ptr(contrib_sum), B.ptr(contrib_count)
+        st = B.stream_of(means2d)
+        B.call("tg_rasterize_fwd", st, B.lib().tg_rasterize_fwd, ctypes.byref(a), st)
+        ctx.save_for_backward(means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, m,
+                              tex_store, tex_scales, isect_offsets, flatten_ids, render_colors, render_alphas,
+                              last_ids, median_ids)
+        ctx.cfg = (range_x, range_y, width, height, tile_size, absgrad, g_weight, adjoint, bg_grad_index_ok,
+                   gs_contrib_threshold)
+        ctx.mark_non_differentiable(contrib_sum, contrib_count)
+        return render_colors, render_alphas, render_normals, render_distort, render_median, contrib_sum, contrib_count
+
+    @staticmethod
+    def backward(ctx, v_render_colors, v_render_alphas, v_render_normals, v_render_distort, v_render_median,
+                 v_contrib_sum, v_contrib_count):
+        (means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, m, tex_store, tex_scales,
+         isect_offsets, flatten_ids, render_colors, render_alphas, last_ids, median_ids) = ctx.saved_tensors
+        (range_x, range_y, width, height, tile_size, absgrad, g_weight, adjoint, bg_grad_index_ok,
+         gs_contrib_threshold) = ctx.cfg
+        dev = means2d.device
+        C, N = isect_offsets.shape[0], means2d.shape[1]
+        D = colors.shape[-1]
+
+        def g(t, shape):
+            return torch.zeros(shape, dtype=torch.float32, device=dev) if t is None else t.float().contiguous()
+
+        v_rc = g(v_render_colors, (C, height, width, D))
+        v_ra = g(v_render_alphas, (C, height, width, 1))
+        v_rn = g(v_render_normals, (C, height, width, 3))
+        v_rd = g(v_render_distort, (C, height, width, 1))
+        v_rm = g(v_render_median, (C, height, width, 1))
+        f = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
+                      backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, None, N, 0.0, g_weight,
+                      C, N)
+        v_means2d = torch.empty_like(means2d)
+        v_means2d_abs = torch.empty_like(means2d) if absgrad else None
+        v_ray_transforms = torch.empty_like(ray_transforms)
+        v_colors = torch.empty_like(colors)
+        v_opacities = torch.empty_like(opacities)
+        v_normals = torch.empty_like(normals)
+        want_tex = tex_store is not None and ctx.needs_input_grad[4]
+        v_textures = torch.empty(textures.shape, dtype=torch.float32, device=dev) if want_tex else None
+        v_densify = torch.empty_like(densify)
+        a = B.RasterBwdArgs(f, B.ptr(render_colors), B.ptr(render_alphas), B.ptr(last_ids), B.ptr(median_ids),
+                            B.ptr(v_rc), B.ptr(v_ra), B.ptr(v_rn), B.ptr(v_rd), B.ptr(v_rm), int(adjoint),
+                            means2d.shape[0] * means2d.shape[1], B.ptr(v_means2d), B.ptr(v_means2d_abs),
+                            B.ptr(v_ray_transforms), B.ptr(v_colors), B.ptr(v_opacities), B.ptr(v_normals),
+                            B.ptr(v_textures), B.ptr(v_densify))
+        st = B.stream_of(means2d)
+        B.call("tg_rasterize_bwd", st, B.lib().tg_rasterize_bwd, ctypes.byref(a), st)
+        if absgrad:
+            means2d.absgrad = v_means2d_abs
+        v_backgrounds = None
+        if bg_grad_index_ok and backgrounds is not None and ctx.needs_input_grad[7]:
+            v_backgrounds = (v_rc * (1.0 - render_alphas).float()).sum(dim=(1, 2))
+        if v_textures is not None and textures.dtype != torch.float32:
+            v_textures = v_textures.to(textures.dtype)
+        return (v_means2d, v_ray_transforms, v_colors, v_opacities, v_textures, v_normals, v_densify, v_backgrounds,
+                None, None, None, None, None, None, None, None, None, None, None, None, None, None, None)
+
+
+def _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
+                  backgrounds, packed):
+    C = isect_offsets.size(0)
+    if packed:
+        nnz = means2d.size(0)
+        assert means2d.shape == (nnz, 2), means2d.shape
+        assert ray_transforms.shape == (nnz, 3, 3), ray_transforms.shape
+        assert colors.shape[0] == nnz, colors.shape
+        assert opacities.shape == (nnz,), opacities.shape
+    else:
+        N = means2d.size(1)
+        assert means2d.shape == (C, N, 2), means2d.shape
+        assert ray_transforms.shape == (C, N, 3, 3), ray_transforms.shape
+        assert colors.shape[:2] == (C, N), colors.shape
+        assert opacities.shape == (C, N), opacities.shape
+    if backgrounds is not None:
+        assert backgrounds.shape == (C, colors.shape[-1]), backgrounds.shape
+    tile_height, tile_width = isect_offsets.shape[1:3]
+    assert tile_height * tile_size >= image_height, f"Assert Failed: {tile_height} * {tile_size} >= {image_height}"
+    assert tile_width * tile_size >= image_width, f"Assert Failed: {tile_width} * {tile_size} >= {image_width}"
+
+
+def rasterize_to_pixels_textured_gaussians(
+    means2d: Tensor,
+    ray_transforms: Tensor,
+    colors: Tensor,
+    opacities: Tensor,
+    textures: Tensor,
+    texture_range_x: float,
+    texture_range_y: float,
+    normals: Tensor,
+    densify: Tensor,
+    image_width: int,
+    image_height: int,
+    tile_size: int,
+    isect_offsets: Tensor,
+    flatten_ids: Tensor,
+    backgrounds: Optional[Tensor] = None,
+    masks: Optional[Tensor] = None,
+    packed: bool = False,
+    absgrad: bool = False,
+    distloss: bool = False,
+    gs_contrib_threshold: float = 0.0,
+    filtering: str = "bilinear",
+    g_weight: float = 1.0,
+    *,
+    texture_storage: Optional[Tensor] = None,
+    texture_scales: Optional[Tensor] = None,
+) -> Tuple[Tensor, ...]:
+    """Rasterize textured 2D Gaussians to pixels (reference: cuda/_wrapper.py:1806-2002).
+
+    Returns the reference's 7-tuple ``(render_colors, render_alphas,
+    render_normals, render_distort, render_median, gs_contrib_sum,
+    gs_contrib_count)``.  ``texture_storage`` (BF16 / FP16 / FP8-E4M3, same
+    [N, th, tw, 4] layout, plus ``texture_scales`` [N] for FP8) is sampled in
+    place of ``textures``; gradients still flow to ``textures`` in FP32.
+    """
+    _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
+                  backgrounds, packed)
+    if filtering not in _FILTER_ADJOINT:
+        raise Exception(f"Unsupported filter type {filtering}")
+    assert textures.dim() == 4 and textures.shape[-1] == 4, textures.shape
+    colors, backgrounds, padded = _pad_channels(colors, backgrounds)
+    store = textures if texture_storage is None else texture_storage
+    store = store.contiguous()
+    if store.dtype == torch.float8_e4m3fn:
+        assert texture_scales is not None, "FP8 texture storage needs texture_scales"
+        texture_scales = texture_scales.float().contiguous()
+    if store.dtype == torch.float64:
+        store = store.float()
+    out = _RasterizeToPixelsTextured.apply(
+        means2d.contiguous(), ray_transforms.contiguous(), colors.contiguous().float(), opacities.contiguous(),
+        textures, normals.contiguous(), densify.contiguous(),
+        None if backgrounds is None else backgrounds.contiguous(), masks, store, texture_scales,
+        float(texture_range_x), float(texture_range_y), int(image_width), int(image_height), int(tile_size),
+        isect_offsets.contiguous(), flatten_ids.contiguous(), absgrad, gs_contrib_threshold, g_weight,
+        _FILTER_ADJOINT[filtering], False)
+    render_colors = out[0]
+    if padded > 0:
+        render_colors = render_colors[..., :-padded]
+    return (render_colors,) + tuple(out[1:])
+
+
+def rasterize_to_pixels_2dgs(
+    means2d: Tensor,
+    ray_transforms: Tensor,
+    colors: Tensor,
+    opacities: Tensor,
+    normals: Tensor,
+    densify: Tensor,
+    image_width: int,
+    image_height: int,
+    tile_size: int,
+    isect_offsets: Tensor,
+    flatten_ids: Tensor,
+    backgrounds: Optional[Tensor] = None,
+    masks: Optional[Tensor] = None,
+    packed: bool = False,
+    absgrad: bool = False,
+    distloss: bool = False,
+    gs_contrib_threshold: float = 0.0,
+) -> Tuple[Tensor, ...]:
+    """Rasterize plain 2D Gaussians to pixels (reference: cuda/_wrapper.py:1647-1784).
+
+    Same 7-tuple as the textured form; the background gradient is computed
+    when the backgrounds require it (reference: cuda/_wrapper.py:2920-2925).
+    """
+    _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
+                  backgrounds, packed)
+    colors, backgrounds, padded = _pad_channels(colors, backgrounds)
+    dummy = torch.empty((0, 1, 1, 4), dtype=torch.float32, device=means2d.device)
+    out = _RasterizeToPixelsTextured.apply(
+        means2d.contiguous(), ray_transforms.contiguous(), colors.contiguous().float(), opacities.contiguous(), dummy,
+        normals.contiguous(), densify.contiguous(), None if backgrounds is None else backgrounds.contiguous(), masks,
+        None, None, 3.0, 3.0, int(image_width), int(image_height), int(tile_size), isect_offsets.contiguous(),
+        flatten_ids.contiguous(), absgrad, gs_contrib_threshold, 1.0, B.TG_ADJ_REFERENCE, True)
+    render_colors = out[0]
+    if padded > 0:
+        render_colors = render_colors[..., :-padded]
+    return (render_colors,) + tuple(out[1:])
