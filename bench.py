@@ -200,6 +200,13 @@ def run_ours(args):
     rank, world, local = dist_setup()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    # one explicit stream for torch ops, library kernels and timing events alike
+    with torch.cuda.stream(torch.cuda.Stream(dev)):
+        _run_ours(args, rank, world, local, dev)
+
+
+def _run_ours(args, rank, world, local, dev):
+    import torch
     from textured_gaussians_b200 import _backend as B
     from textured_gaussians_b200 import rasterization_textured_gaussians
     from textured_gaussians_b200.cuda import make_texture_storage
