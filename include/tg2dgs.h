@@ -134,6 +134,20 @@ TG_API size_t tg_sort_workspace_bytes(int64_t n, int32_t end_bit);
 TG_API int tg_sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, int64_t n, int32_t end_bit,
                   void* workspace, size_t workspace_bytes, int32_t* result_in_alt, tg_stream_t stream);
 
+/* The same sort, for callers that cannot allocate device memory (a plugin host
+ * that owns all GPU memory, a real-time loop that must not call cudaMalloc, a
+ * host without a caching allocator).  No counterpart in the reference.  The
+ * caller passes only keys, values and their ping-pong buffers; the scratch the
+ * sort needs lives in a static device array of this library (8 MiB + 16 KiB
+ * held on every GPU that loads it, until exit), so n is limited to
+ * TG_SORT_NOALLOC_MAX_PAIRS -- larger n is rejected with TG_ERR_INVALID_ARG.
+ * Calls share that array: those that overlap on one GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the array's
+ * address with that device current; make it before any stream capture. */
+#define TG_SORT_NOALLOC_MAX_PAIRS 4194304
+TG_API int tg_sort_pairs_noalloc(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, int64_t n,
+                                 int32_t end_bit, int32_t* result_in_alt, tg_stream_t stream);
+
 /* Replaces isect_offset_encode_tensor (textured_gaussians/cuda/csrc/isect_tiles.cu:357-390):
  * offsets[c,ty,tx] = index of the first sorted intersection of tile (c,ty,tx)
  * or of the next non-empty tile. */

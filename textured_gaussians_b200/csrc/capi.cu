@@ -30,6 +30,7 @@ cudaError_t launch_sh_fwd(int64_t n, int64_t rows, int degree, int K, const floa
 cudaError_t launch_sh_bwd(int64_t n, int64_t rows, int degree, int K, const float* dirs, const float* coeffs,
                           const uint8_t* masks, const float* v_colors, float* v_coeffs, float* v_dirs,
                           cudaStream_t s);
+int fail_with(int code, const char* msg);
 }  // namespace tg
 
 namespace {
@@ -62,6 +63,12 @@ int bit_width(int64_t n) {  // floor(log2(n)) + 1, as the reference computes it
     while (n > 0) { ++b; n >>= 1; }
     return b;
 }
+
+}  // namespace
+
+int tg::fail_with(int code, const char* msg) { return fail(code, "%s", msg); }
+
+namespace {
 
 #define TG_REQUIRE(cond, code, ...) \
     do {                            \
