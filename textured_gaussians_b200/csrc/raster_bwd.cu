@@ -53,15 +53,159 @@ struct GradSlots {
     static constexpr int kCount = D + 17;
 };
 
+// Resident CTAs per SM the register allocation targets.
+#ifndef TG_BWD_MIN_CTAS
+#define TG_BWD_MIN_CTAS 2
+#endif
+// Pixels per thread for 16x16 tiles.
+#ifndef TG_BWD_PPT
+#define TG_BWD_PPT 1
+#endif
+
+// Per-pixel state of the back-to-front sweep.
+template <int D>
+struct PixelAdj {
+    int64_t pix;
+    float px, py;
+    bool inside;
+    float T_final, T, v_a, v_dist, v_med, bg_dot;
+    float v_c[D], buf[D];
+    float v_n[3], buf_n[3];
+    int32_t bin_final, median_idx;
+    float acc_d_buf, acc_d, acc_w_buf, acc_w, dist_buf;
+};
+
+// Adds one (pixel, splat) pair's gradient contributions to the lane's per-splat
+// sums `vals` (slots of GradSlots<D>), issues the pair's texel-gradient atomics,
+// and advances the pixel's back-to-front state.  Follows
+// rasterize_to_pixels_textured_gaussians_2dgs_bwd.cu:438-627 (+ bwd2.cu:612-676).
 template <int D, class Tex>
-__global__ void __launch_bounds__(256) raster_bwd_kernel(const tg_raster_bwd_args a, const float uv_scale) {
+__device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, const PairEval& e, PixelAdj<D>& P,
+                                                const float4 xyo, const float4 nn, const float* cp, int32_t idx,
+                                                float* vt, float uv_scale, float (&vals)[32]) {
     constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
+    using GS = GradSlots<D>;
+    const tg_raster_fwd_args& f = a.f;
+    const float opac = xyo.z;
+    if (idx == P.median_idx) vals[GS::kRgb + D - 1] += P.v_med;
+    const float ra = 1.f / (1.f - e.alpha);
+    P.T *= ra;
+    const float T = P.T;
+    const float fac = e.alpha * T;
+    float texc[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        vals[GS::kRgb + k] += fac * P.v_c[k];
+        texc[k] = kTextured ? tex_color(e, k) : 0.f;
+    }
+    float v_alpha = 0.f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) v_alpha += ((texc[k] + cp[k]) * T - P.buf[k] * ra) * P.v_c[k];
+    vals[GS::kNrm + 0] += fac * P.v_n[0];
+    vals[GS::kNrm + 1] += fac * P.v_n[1];
+    vals[GS::kNrm + 2] += fac * P.v_n[2];
+    v_alpha += (nn.x * T - P.buf_n[0] * ra) * P.v_n[0];
+    v_alpha += (nn.y * T - P.buf_n[1] * ra) * P.v_n[1];
+    v_alpha += (nn.z * T - P.buf_n[2] * ra) * P.v_n[2];
+    v_alpha += P.T_final * ra * P.v_a;
+    if (f.backgrounds) v_alpha += -P.T_final * ra * P.bg_dot;
+    {
+        const float depth = cp[D - 1];
+        const float dl_dw = 2.f * (2.f * (depth * P.acc_w_buf - P.acc_d_buf) + (P.acc_d - depth * P.acc_w));
+        v_alpha += (dl_dw * T - P.dist_buf * ra) * P.v_dist;
+        P.acc_d_buf -= fac * depth;
+        P.acc_w_buf -= fac;
+        P.dist_buf += dl_dw * fac;
+        vals[GS::kRgb + D - 1] += 2.f * fac * (2.f - 2.f * T - P.acc_w + fac) * P.v_dist;
+    }
+    // d L / d s, from the Gaussian kernel (3D branch) and, for the UV-aware adjoints, from the
+    // texture lookup; both go back through s = zeta.xy / zeta.z and zeta = h_u x h_v once
+    float vsx = 0.f, vsy = 0.f;
+    const bool unclamped = kTextured ? (opac * e.vis * e.asf <= 0.999f) : (opac * e.vis <= 0.999f);
+    float tex_a_grad = 0.f;  // d L / d (texture alpha) / w_i
+    if (unclamped) {
+        const float v_G = kTextured ? opac * v_alpha * e.asf : opac * v_alpha;
+        const float dG = kTextured ? -f.g_weight * e.kern : -e.vis;
+        if (e.g3 <= e.g2) {
+            vsx = v_G * dG * e.sx;
+            vsy = v_G * dG * e.sy;
+        } else {
+            const float vx = v_G * (dG * kFilterInvSquare * e.dx);
+            const float vy = v_G * (dG * kFilterInvSquare * e.dy);
+            vals[GS::kXY] += vx;
+            vals[GS::kXY + 1] += vy;
+            vals[GS::kAbs] += fabsf(vx);
+            vals[GS::kAbs + 1] += fabsf(vy);
+        }
+        vals[GS::kOpac] += kTextured ? e.vis * v_alpha * e.asf : e.vis * v_alpha;
+        tex_a_grad = e.vis * opac * v_alpha;
+    }
+    if (kTextured && e.tex_valid && vt != nullptr) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float4 gq;
+            gq.x = 0 < D ? fac * e.w[q] * P.v_c[0] : 0.f;
+            gq.y = 1 < D ? fac * e.w[q] * P.v_c[1 < D ? 1 : 0] : 0.f;
+            gq.z = 2 < D ? fac * e.w[q] * P.v_c[2 < D ? 2 : 0] : 0.f;
+            gq.w = (3 < D ? fac * e.w[q] * P.v_c[3 < D ? 3 : 0] : 0.f) + e.w[q] * tex_a_grad;
+            if (gq.x != 0.f || gq.y != 0.f || gq.z != 0.f || gq.w != 0.f)
+                atomicAdd(reinterpret_cast<float4*>(vt + 4 * (int64_t)e.toff[q]), gq);
+        }
+    }
+    if (kTextured && e.tex_valid && uv_scale != 0.f) {
+        const float wu = e.w[1] + e.w[3], wv = e.w[2] + e.w[3];
+        const float dbu[4] = {-(1.f - wv), 1.f - wv, -wv, wv};
+        const float dbv[4] = {-(1.f - wu), -wu, 1.f - wu, wu};
+        const float du = uv_scale * (float)(f.tex_rx - 1) / f.range_x;
+        const float dv = uv_scale * (float)(f.tex_ry - 1) / f.range_y;
+        float tsx = 0.f, tsy = 0.f;
+#pragma unroll
+        for (int k = 0; k < D && k < 4; ++k) {
+            const float vt_k = fac * P.v_c[k];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float tv = f4get(e.tx[q], k);
+                tsx += vt_k * dbu[q] * tv;
+                tsy += vt_k * dbv[q] * tv;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            tsx += tex_a_grad * dbu[q] * e.tx[q].w;
+            tsy += tex_a_grad * dbv[q] * e.tx[q].w;
+        }
+        vsx += tsx * du;
+        vsy += tsy * dv;
+    }
+    if (vsx != 0.f || vsy != 0.f) {
+        const float iz = 1.f / e.z.z;
+        const float a_ = vsx * iz, b_ = vsy * iz;
+        const f3 vz = mk3(a_, b_, -(a_ * e.sx + b_ * e.sy));
+        const f3 vhu = cross(e.hv, vz), vhv = cross(vz, e.hu);
+        vals[GS::kM + 0] -= vhu.x; vals[GS::kM + 1] -= vhu.y; vals[GS::kM + 2] -= vhu.z;
+        vals[GS::kM + 3] -= vhv.x; vals[GS::kM + 4] -= vhv.y; vals[GS::kM + 5] -= vhv.z;
+        vals[GS::kM + 6] += P.px * vhu.x + P.py * vhv.x;
+        vals[GS::kM + 7] += P.px * vhu.y + P.py * vhv.y;
+        vals[GS::kM + 8] += P.px * vhu.z + P.py * vhv.z;
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k) P.buf[k] += (texc[k] + cp[k]) * fac;
+    P.buf_n[0] += nn.x * fac;
+    P.buf_n[1] += nn.y * fac;
+    P.buf_n[2] += nn.z * fac;
+}
+
+template <int D, class Tex, int PPT>
+__global__ void __launch_bounds__(256 / PPT, TG_BWD_MIN_CTAS) raster_bwd_kernel(const tg_raster_bwd_args a,
+                                                                                const float uv_scale) {
     using GS = GradSlots<D>;
     constexpr int NV = GS::kCount;
     const tg_raster_fwd_args& f = a.f;
     extern __shared__ float4 smem4[];
-    const int bs = blockDim.x;
-    float4* s_xyo = smem4;
+    const int nt = blockDim.x;
+    const int bs = nt * PPT;  // splats per batch = tile_size^2
+    float4* s_box = smem4;  // per-splat cull box (see cull_box)
+    float4* s_xyo = s_box + bs;
     float4* s_m0 = s_xyo + bs;
     float4* s_m1 = s_m0 + bs;
     float4* s_m2 = s_m1 + bs;
@@ -79,50 +223,73 @@ __global__ void __launch_bounds__(256) raster_bwd_kernel(const tg_raster_bwd_arg
     if (f.masks != nullptr && !f.masks[(int64_t)tc.c * per_cam + tc.tile]) return;
 
     const int ts = f.tile_size;
-    const int i = tc.ty * ts + tr / ts;
-    const int j = tc.tx * ts + tr % ts;
-    const bool inside = i < f.height && j < f.width;
-    const int64_t pix = ((int64_t)tc.c * f.height + i) * f.width + j;
     const int64_t toff = (int64_t)tc.c * per_cam + tc.tile;
     const int32_t range_start = f.tile_offsets[toff];
     const int32_t range_end = (tc.c == f.C - 1 && tc.tile == per_cam - 1) ? (int32_t)f.n_isects : f.tile_offsets[toff + 1];
 
-    for (int k = tr; k < bs * NV; k += bs) s_grad[k] = 0.f;
+    // pixel-centre rectangle covered by this warp (for the warp-level cull)
+    float wx0 = INFINITY, wx1 = -INFINITY, wy0 = INFINITY, wy1 = -INFINITY;
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+        const int local = tr + q * nt;
+        const float cx = (float)(tc.tx * ts + local % ts) + 0.5f, cy = (float)(tc.ty * ts + local / ts) + 0.5f;
+        wx0 = fminf(wx0, cx); wx1 = fmaxf(wx1, cx); wy0 = fminf(wy0, cy); wy1 = fmaxf(wy1, cy);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        wx0 = fminf(wx0, __shfl_xor_sync(wmask, wx0, o)); wx1 = fmaxf(wx1, __shfl_xor_sync(wmask, wx1, o));
+        wy0 = fminf(wy0, __shfl_xor_sync(wmask, wy0, o)); wy1 = fmaxf(wy1, __shfl_xor_sync(wmask, wy1, o));
+    }
+    for (int k = tr; k < bs * NV; k += nt) s_grad[k] = 0.f;
     if (tr == 0) s_max_bin = -1;
 
-    const float px = (float)j + 0.5f, py = (float)i + 0.5f;
-    float T_final = 1.f, v_a = 0.f, v_dist = 0.f, v_med = 0.f, bg_dot = 0.f;
-    float v_c[D], buf[D];
-    float v_n[3] = {0.f, 0.f, 0.f}, buf_n[3] = {0.f, 0.f, 0.f};
-    int32_t bin_final = -1, median_idx = -1;
-    float acc_d_buf = 0.f, acc_d = 0.f, acc_w_buf = 0.f, acc_w = 0.f, dist_buf = 0.f;
+    PixelAdj<D> P[PPT];
+    int32_t thread_bin = -1;
 #pragma unroll
-    for (int k = 0; k < D; ++k) { v_c[k] = 0.f; buf[k] = 0.f; }
-    if (inside) {
-        const float alpha_out = a.render_alphas[pix];
-        T_final = 1.f - alpha_out;
-        bin_final = a.last_ids[pix];
-        median_idx = a.median_ids[pix];
+    for (int q = 0; q < PPT; ++q) {
+        PixelAdj<D>& p = P[q];
+        const int local = tr + q * nt;
+        const int i = tc.ty * ts + local / ts;
+        const int j = tc.tx * ts + local % ts;
+        p.inside = i < f.height && j < f.width;
+        p.pix = ((int64_t)tc.c * f.height + i) * f.width + j;
+        p.px = (float)j + 0.5f;
+        p.py = (float)i + 0.5f;
+        p.T_final = 1.f; p.v_a = p.v_dist = p.v_med = p.bg_dot = 0.f;
+        p.bin_final = -1; p.median_idx = -1;
+        p.acc_d_buf = p.acc_d = p.acc_w_buf = p.acc_w = p.dist_buf = 0.f;
+        p.v_n[0] = p.v_n[1] = p.v_n[2] = 0.f;
+        p.buf_n[0] = p.buf_n[1] = p.buf_n[2] = 0.f;
 #pragma unroll
-        for (int k = 0; k < D; ++k) v_c[k] = a.v_render_colors[pix * D + k];
-        v_a = a.v_render_alphas[pix];
-        v_n[0] = a.v_render_normals[pix * 3];
-        v_n[1] = a.v_render_normals[pix * 3 + 1];
-        v_n[2] = a.v_render_normals[pix * 3 + 2];
-        v_dist = a.v_render_distort[pix];
-        v_med = a.v_render_median[pix];
-        acc_d_buf = a.render_colors[pix * D + D - 1];
-        acc_d = acc_d_buf;
-        acc_w_buf = alpha_out;
-        acc_w = alpha_out;
-        if (f.backgrounds) {
+        for (int k = 0; k < D; ++k) { p.v_c[k] = 0.f; p.buf[k] = 0.f; }
+        if (p.inside) {
+            const int64_t px_ = p.pix;
+            const float alpha_out = a.render_alphas[px_];
+            p.T_final = 1.f - alpha_out;
+            p.bin_final = a.last_ids[px_];
+            p.median_idx = a.median_ids[px_];
 #pragma unroll
-            for (int k = 0; k < D; ++k) bg_dot += f.backgrounds[tc.c * D + k] * v_c[k];
+            for (int k = 0; k < D; ++k) p.v_c[k] = a.v_render_colors[px_ * D + k];
+            p.v_a = a.v_render_alphas[px_];
+            p.v_n[0] = a.v_render_normals[px_ * 3];
+            p.v_n[1] = a.v_render_normals[px_ * 3 + 1];
+            p.v_n[2] = a.v_render_normals[px_ * 3 + 2];
+            p.v_dist = a.v_render_distort[px_];
+            p.v_med = a.v_render_median[px_];
+            p.acc_d_buf = a.render_colors[px_ * D + D - 1];
+            p.acc_d = p.acc_d_buf;
+            p.acc_w_buf = alpha_out;
+            p.acc_w = alpha_out;
+            if (f.backgrounds) {
+#pragma unroll
+                for (int k = 0; k < D; ++k) p.bg_dot += f.backgrounds[tc.c * D + k] * p.v_c[k];
+            }
         }
+        p.T = p.T_final;
+        thread_bin = max(thread_bin, p.bin_final);
     }
-    float T = T_final;
-    // last contributor over the warp and over the CTA
-    const int32_t warp_bin_final = __reduce_max_sync(wmask, bin_final);  // uniform across the warp
+    // last contributor over the warp (uniform) and over the CTA
+    const int32_t warp_bin_final = __reduce_max_sync(wmask, thread_bin);
     __syncthreads();
     if (lane == __ffs(wmask) - 1) atomicMax(&s_max_bin, warp_bin_final);
     __syncthreads();
@@ -133,158 +300,62 @@ __global__ void __launch_bounds__(256) raster_bwd_kernel(const tg_raster_bwd_arg
         if (batch_end - (bs - 1) > block_max_bin) continue;  // every splat here is past all last contributors
         const int32_t batch_size = min(bs, batch_end + 1 - range_start);
         __syncthreads();  // previous batch fully flushed before restaging
-        const int32_t idx_load = batch_end - tr;
-        if (idx_load >= range_start) {
-            const int32_t g = f.flatten_ids[idx_load];
-            const float2 xy = reinterpret_cast<const float2*>(f.means2d)[g];
-            const int32_t row = f.gaussian_ids ? (int32_t)f.gaussian_ids[g] : g % f.N;
-            const float scale = (Tex::kFormat == TG_TEX_FP8_E4M3) ? f.tex_scales[row] : 1.f;
-            s_xyo[tr] = make_float4(xy.x, xy.y, f.opacities[g], scale);
-            const float* m = f.ray_transforms + 9 * (int64_t)g;
-            s_m0[tr] = make_float4(m[0], m[1], m[2], 0.f);
-            s_m1[tr] = make_float4(m[3], m[4], m[5], 0.f);
-            s_m2[tr] = make_float4(m[6], m[7], m[8], 0.f);
-            const float* n = f.normals + 3 * (int64_t)g;
-            s_nrm[tr] = make_float4(n[0], n[1], n[2], 0.f);
 #pragma unroll
-            for (int k = 0; k < D; ++k) s_col[tr * D + k] = f.colors[(int64_t)g * D + k];
-            s_row[tr] = row;
-            s_g[tr] = g;
+        for (int q = 0; q < PPT; ++q) {
+            const int slot = tr + q * nt;
+            const int32_t idx_load = batch_end - slot;
+            if (idx_load >= range_start) {
+                const int32_t g = f.flatten_ids[idx_load];
+                const float2 xy = reinterpret_cast<const float2*>(f.means2d)[g];
+                const int32_t row = f.gaussian_ids ? (int32_t)f.gaussian_ids[g] : g % f.N;
+                const float scale = (Tex::kFormat == TG_TEX_FP8_E4M3) ? f.tex_scales[row] : 1.f;
+                s_xyo[slot] = make_float4(xy.x, xy.y, f.opacities[g], scale);
+                const float* m = f.ray_transforms + 9 * (int64_t)g;
+                s_m0[slot] = make_float4(m[0], m[1], m[2], 0.f);
+                s_m1[slot] = make_float4(m[3], m[4], m[5], 0.f);
+                s_m2[slot] = make_float4(m[6], m[7], m[8], 0.f);
+                s_box[slot] = cull_box(s_xyo[slot], s_m0[slot], s_m1[slot], s_m2[slot], Tex::kFormat != TG_TEX_NONE,
+                                       f.range_x, f.range_y, f.g_weight);
+                const float* n = f.normals + 3 * (int64_t)g;
+                s_nrm[slot] = make_float4(n[0], n[1], n[2], 0.f);
+#pragma unroll
+                for (int k = 0; k < D; ++k) s_col[slot * D + k] = f.colors[(int64_t)g * D + k];
+                s_row[slot] = row;
+                s_g[slot] = g;
+            }
         }
         __syncthreads();
         for (int t = max(0, batch_end - warp_bin_final); t < batch_size; ++t) {
             const int32_t idx = batch_end - t;
-            bool valid = inside && idx <= bin_final;
-            PairEval e;
-            const float4 xyo = s_xyo[t];
+            const float4 box = s_box[t];
+            if (box.z < wx0 || box.x > wx1 || box.w < wy0 || box.y > wy1) continue;  // no pixel of this warp can be valid
+            const float4 xyo = s_xyo[t], m0 = s_m0[t], m1 = s_m1[t], m2 = s_m2[t];
             const int row = s_row[t];
-            if (valid) {
-                eval_pair<Tex>(e, px, py, xyo, s_m0[t], s_m1[t], s_m2[t], f.textures, (int64_t)row * tex_stride,
-                               f.tex_rx, f.tex_ry, f.range_x, f.range_y, f.g_weight);
-                valid = e.valid;
-            }
-            if (!__any_sync(wmask, valid)) continue;
+            const int64_t tex_base = (int64_t)row * tex_stride;
+            const float4 nn = s_nrm[t];
+            const float* cp = s_col + t * D;
+            float* vt = a.v_textures != nullptr ? a.v_textures + 4 * tex_base : nullptr;
             float vals[32];
 #pragma unroll
             for (int k = 0; k < 32; ++k) vals[k] = 0.f;
-            if (valid) {
-                const float opac = xyo.z;
-                const float* cp = s_col + t * D;
-                const float4 nn = s_nrm[t];
-                if (idx == median_idx) vals[GS::kRgb + D - 1] += v_med;
-                const float ra = 1.f / (1.f - e.alpha);
-                T *= ra;
-                const float fac = e.alpha * T;
-                float texc[D];
+            bool any = false;
 #pragma unroll
-                for (int k = 0; k < D; ++k) {
-                    vals[GS::kRgb + k] += fac * v_c[k];
-                    texc[k] = kTextured ? tex_color(e, k) : 0.f;
-                }
-                float v_alpha = 0.f;
-#pragma unroll
-                for (int k = 0; k < D; ++k) v_alpha += ((texc[k] + cp[k]) * T - buf[k] * ra) * v_c[k];
-                vals[GS::kNrm + 0] = fac * v_n[0];
-                vals[GS::kNrm + 1] = fac * v_n[1];
-                vals[GS::kNrm + 2] = fac * v_n[2];
-                v_alpha += (nn.x * T - buf_n[0] * ra) * v_n[0];
-                v_alpha += (nn.y * T - buf_n[1] * ra) * v_n[1];
-                v_alpha += (nn.z * T - buf_n[2] * ra) * v_n[2];
-                v_alpha += T_final * ra * v_a;
-                if (f.backgrounds) v_alpha += -T_final * ra * bg_dot;
-                {
-                    const float depth = cp[D - 1];
-                    const float dl_dw = 2.f * (2.f * (depth * acc_w_buf - acc_d_buf) + (acc_d - depth * acc_w));
-                    v_alpha += (dl_dw * T - dist_buf * ra) * v_dist;
-                    acc_d_buf -= fac * depth;
-                    acc_w_buf -= fac;
-                    dist_buf += dl_dw * fac;
-                    vals[GS::kRgb + D - 1] += 2.f * fac * (2.f - 2.f * T - acc_w + fac) * v_dist;
-                }
-                f3 vM0 = mk3(0, 0, 0), vM1 = mk3(0, 0, 0), vM2 = mk3(0, 0, 0);
-                const bool unclamped = kTextured ? (opac * e.vis * e.asf <= 0.999f) : (opac * e.vis <= 0.999f);
-                float tex_a_grad = 0.f;  // d L / d (texture alpha) / w_i
-                if (unclamped) {
-                    const float v_G = kTextured ? opac * v_alpha * e.asf : opac * v_alpha;
-                    const float dG = kTextured ? -f.g_weight * e.kern : -e.vis;
-                    if (e.g3 <= e.g2) {
-                        const float vsx = v_G * dG * e.sx, vsy = v_G * dG * e.sy;
-                        const float a_ = vsx / e.z.z, b_ = vsy / e.z.z;
-                        const f3 vz = mk3(a_, b_, -(a_ * e.sx + b_ * e.sy));
-                        const f3 vhu = cross(e.hv, vz), vhv = cross(vz, e.hu);
-                        vM0 = -1.f * vhu;
-                        vM1 = -1.f * vhv;
-                        vM2 = px * vhu + py * vhv;
-                    } else {
-                        const float vx = v_G * (dG * kFilterInvSquare * e.dx);
-                        const float vy = v_G * (dG * kFilterInvSquare * e.dy);
-                        vals[GS::kXY] = vx;
-                        vals[GS::kXY + 1] = vy;
-                        vals[GS::kAbs] = fabsf(vx);
-                        vals[GS::kAbs + 1] = fabsf(vy);
-                    }
-                    vals[GS::kOpac] = kTextured ? e.vis * v_alpha * e.asf : e.vis * v_alpha;
-                    tex_a_grad = e.vis * opac * v_alpha;
-                }
-                if (kTextured && e.tex_valid && a.v_textures != nullptr) {
-                    float* vt = a.v_textures + 4 * ((int64_t)row * tex_stride);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        float4 gq;
-                        gq.x = 0 < D ? fac * e.w[q] * v_c[0] : 0.f;
-                        gq.y = 1 < D ? fac * e.w[q] * v_c[1 < D ? 1 : 0] : 0.f;
-                        gq.z = 2 < D ? fac * e.w[q] * v_c[2 < D ? 2 : 0] : 0.f;
-                        gq.w = (3 < D ? fac * e.w[q] * v_c[3 < D ? 3 : 0] : 0.f) + e.w[q] * tex_a_grad;
-                        if (gq.x != 0.f || gq.y != 0.f || gq.z != 0.f || gq.w != 0.f)
-                            atomicAdd(reinterpret_cast<float4*>(vt + 4 * (int64_t)e.toff[q]), gq);
-                    }
-                    if (uv_scale != 0.f) {
-                        const float wu = e.w[1] + e.w[3], wv = e.w[2] + e.w[3];
-                        const float dbu[4] = {-(1.f - wv), 1.f - wv, -wv, wv};
-                        const float dbv[4] = {-(1.f - wu), -wu, 1.f - wu, wu};
-                        const float du = uv_scale * (float)(f.tex_rx - 1) / f.range_x;
-                        const float dv = uv_scale * (float)(f.tex_ry - 1) / f.range_y;
-                        float tsx = 0.f, tsy = 0.f;
-#pragma unroll
-                        for (int k = 0; k < D && k < 4; ++k) {
-                            const float vt_k = fac * v_c[k];
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                const float tv = f4get(e.tx[q], k);
-                                tsx += vt_k * dbu[q] * tv * du;
-                                tsy += vt_k * dbv[q] * tv * dv;
-                            }
-                        }
-                        if (unclamped) {
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                tsx += tex_a_grad * dbu[q] * e.tx[q].w * du;
-                                tsy += tex_a_grad * dbv[q] * e.tx[q].w * dv;
-                            }
-                        }
-                        const float a_ = tsx / e.z.z, b_ = tsy / e.z.z;
-                        const f3 vz = mk3(a_, b_, -(a_ * e.sx + b_ * e.sy));
-                        const f3 vhu = cross(e.hv, vz), vhv = cross(vz, e.hu);
-                        vM0 = vM0 - vhu;
-                        vM1 = vM1 - vhv;
-                        vM2 = vM2 + (px * vhu + py * vhv);
-                    }
-                }
-                vals[GS::kM + 0] = vM0.x; vals[GS::kM + 1] = vM0.y; vals[GS::kM + 2] = vM0.z;
-                vals[GS::kM + 3] = vM1.x; vals[GS::kM + 4] = vM1.y; vals[GS::kM + 5] = vM1.z;
-                vals[GS::kM + 6] = vM2.x; vals[GS::kM + 7] = vM2.y; vals[GS::kM + 8] = vM2.z;
-#pragma unroll
-                for (int k = 0; k < D; ++k) buf[k] += (texc[k] + cp[k]) * fac;
-                buf_n[0] += nn.x * fac;
-                buf_n[1] += nn.y * fac;
-                buf_n[2] += nn.z * fac;
+            for (int q = 0; q < PPT; ++q) {
+                if (!(P[q].inside && idx <= P[q].bin_final) || !in_box(box, P[q].px, P[q].py)) continue;
+                PairEval e;
+                eval_pair<Tex>(e, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx, f.tex_ry,
+                               f.range_x, f.range_y, f.g_weight);
+                if (!e.valid) continue;
+                any = true;
+                accumulate_pair<D, Tex>(a, e, P[q], xyo, nn, cp, idx, vt, uv_scale, vals);
             }
+            if (!__any_sync(wmask, any)) continue;
             warp_reduce_scatter32(vals, wmask);
             if (lane < NV && vals[0] != 0.f) atomicAdd(s_grad + t * NV + lane, vals[0]);
         }
         __syncthreads();
         // flush this batch's per-splat sums: one global atomic per (splat, value)
-        for (int k = tr; k < batch_size * NV; k += bs) {
+        for (int k = tr; k < batch_size * NV; k += nt) {
             const float v = s_grad[k];
             if (v == 0.f) continue;
             s_grad[k] = 0.f;
@@ -315,16 +386,22 @@ __global__ void densify_grad_kernel(const float* __restrict__ v_M, const float* 
 template <int D, class Tex>
 cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     const tg_raster_fwd_args& f = a.f;
-    const int bs = f.tile_size * f.tile_size;
-    const size_t smem = (size_t)bs * (5 * sizeof(float4) + D * sizeof(float) + 2 * sizeof(int) +
-                                      GradSlots<D>::kCount * sizeof(float));
+    const int tile_px = f.tile_size * f.tile_size;
+    const size_t smem = (size_t)tile_px * (6 * sizeof(float4) + D * sizeof(float) + 2 * sizeof(int) +
+                                           GradSlots<D>::kCount * sizeof(float));
     const int64_t blocks = (int64_t)f.C * f.tile_width * f.tile_height;
     const float uv_scale = a.adjoint == TG_ADJ_BWD2 ? 1.f : (a.adjoint == TG_ADJ_EXACT ? 0.5f : 0.f);
-    cudaError_t err = cudaFuncSetAttribute(raster_bwd_kernel<D, Tex>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem);
+    const bool multi = tile_px >= 64 * TG_BWD_PPT;
+    cudaError_t err = multi ? cudaFuncSetAttribute(raster_bwd_kernel<D, Tex, TG_BWD_PPT>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                            : cudaFuncSetAttribute(raster_bwd_kernel<D, Tex, 1>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     if (blocks > 0 && f.n_isects > 0) {
-        raster_bwd_kernel<D, Tex><<<(unsigned)blocks, bs, smem, s>>>(a, uv_scale);
+        if (multi)
+            raster_bwd_kernel<D, Tex, TG_BWD_PPT><<<(unsigned)blocks, tile_px / TG_BWD_PPT, smem, s>>>(a, uv_scale);
+        else
+            raster_bwd_kernel<D, Tex, 1><<<(unsigned)blocks, tile_px, smem, s>>>(a, uv_scale);
         note_launches(1);
     }
     if ((err = cudaGetLastError()) != cudaSuccess) return err;

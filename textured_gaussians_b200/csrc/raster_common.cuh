@@ -40,16 +40,19 @@ __device__ __forceinline__ void eval_pair(PairEval& e, float px, float py, const
         e.valid = false;
         return;
     }
-    e.sx = e.z.x / e.z.z;
-    e.sy = e.z.y / e.z.z;
+    const float iz = 1.f / e.z.z;
+    e.sx = e.z.x * iz;
+    e.sy = e.z.y * iz;
     if (kTextured) {
         if (!(e.sx < -range_x || e.sx > range_x || e.sy < -range_y || e.sy > range_y)) {
-            float u = (e.sx + range_x) / (range_x * 2.f) * (float)(rx - 1);
-            float v = (e.sy + range_y) / (range_y * 2.f) * (float)(ry - 1);
-            if (u < 0.f) u = 0.f; else if (u > (float)(rx - 1)) u = (float)(rx - 1);
-            if (v < 0.f) v = 0.f; else if (v > (float)(ry - 1)) v = (float)(ry - 1);
-            const int ul = (int)floorf(u), vl = (int)floorf(v), uh = (int)ceilf(u), vh = (int)ceilf(v);
+            // u = (s + range) / (2 range) * (R - 1), clamped to [0, R-1]
+            const float ku = (float)(rx - 1) / (range_x * 2.f), kv = (float)(ry - 1) / (range_y * 2.f);
+            const float u = fminf(fmaxf((e.sx + range_x) * ku, 0.f), (float)(rx - 1));
+            const float v = fminf(fmaxf((e.sy + range_y) * kv, 0.f), (float)(ry - 1));
+            // u >= 0, so truncation is floor; ceil is floor + 1 exactly when u has a fractional part
+            const int ul = (int)u, vl = (int)v;
             const float wu = u - (float)ul, wv = v - (float)vl;
+            const int uh = ul + (wu > 0.f), vh = vl + (wv > 0.f);
             e.w[0] = (1.f - wu) * (1.f - wv);
             e.w[1] = wu * (1.f - wv);
             e.w[2] = (1.f - wu) * wv;
@@ -81,6 +84,68 @@ __device__ __forceinline__ void eval_pair(PairEval& e, float px, float py, const
         e.alpha = fminf(0.999f, xyo.z * e.vis);
     }
     if (sigma < 0.f || e.alpha < 1.f / 255.f) e.valid = false;
+}
+
+// Pixel-space box outside of which a (pixel, splat) pair is provably invalid
+// (alpha < 1/255), so skipping it leaves every output unchanged.
+//
+// A pair is valid only if opac * vis * asf >= 1/255 with
+// vis = 0.998 - g_weight + g_weight exp(-sigma), sigma = min(|s|^2, 2|d|^2) / 2.
+// Outside the texture square |s_x| <= range_x, |s_y| <= range_y the texture
+// alpha scale asf is exactly 1, so validity there needs sigma <= sigma1 with
+// exp(-sigma1) = (1/(255 opac) - 0.998 + g_weight) / g_weight: either the UV
+// point lies in the disk |s|^2 <= 2 sigma1 (inside the square of half-side
+// sqrt(2 sigma1)) or the pixel lies within sqrt(sigma1) of the projected
+// centre.  Inside the texture square anything is possible.  The UV squares map
+// to pixel space through the splat's homography pixel(s) = (M0.(s,1),
+// M1.(s,1)) / M2.(s,1); when M2.(s,1) has one sign at all four corners the
+// image is a bounded convex quadrilateral, whose corners' box bounds it.
+// Otherwise (or if no bound on sigma exists) the box is unbounded.  The box is
+// widened by a margin that covers FP32 rounding of the pair evaluation.
+__device__ __forceinline__ float4 cull_box(const float4 xyo, const float4 m0, const float4 m1, const float4 m2,
+                                           bool textured, float range_x, float range_y, float g_weight) {
+    const float4 all = make_float4(-INFINITY, -INFINITY, INFINITY, INFINITY);
+    const float opac = xyo.z;
+    float K;  // lower bound on exp(-sigma) for a valid pair outside the texture square
+    if (textured) {
+        if (!(g_weight > 0.f)) return all;
+        K = (1.f / (255.f * opac) - 0.998f + g_weight) / g_weight;
+    } else {
+        K = 1.f / (255.f * opac);
+    }
+    K *= 0.999f;  // rounding slack: never cull a pair the evaluation could still accept
+    if (!(K > 0.f)) return all;
+    const float sig1 = K >= 1.f ? 0.f : -logf(K) * 1.001f + 1e-3f;
+    const float rs = sqrtf(2.f * sig1);   // half-side of the UV square around the Gaussian disk
+    const float rd = sqrtf(sig1);         // radius of the 2D-filter disk, pixels
+    const float hx = textured ? fmaxf(rs, range_x) : rs;
+    const float hy = textured ? fmaxf(rs, range_y) : rs;
+    float x0 = xyo.x - rd, x1 = xyo.x + rd, y0 = xyo.y - rd, y1 = xyo.y + rd;
+    int pos = 0, neg = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float u = (c & 1) ? hx : -hx, v = (c & 2) ? hy : -hy;
+        const float X = m0.x * u + m0.y * v + m0.z;
+        const float Y = m1.x * u + m1.y * v + m1.z;
+        const float Z = m2.x * u + m2.y * v + m2.z;
+        pos += Z > 0.f;
+        neg += Z < 0.f;
+        const float iz = 1.f / Z;
+        const float px = X * iz, py = Y * iz;
+        x0 = fminf(x0, px); x1 = fmaxf(x1, px);
+        y0 = fminf(y0, py); y1 = fmaxf(y1, py);
+    }
+    if (!(pos == 4 || neg == 4)) return all;
+    const float margin = 1.f + 1e-3f * ((x1 - x0) + (y1 - y0));
+    const float4 box = make_float4(x0 - margin, y0 - margin, x1 + margin, y1 + margin);
+    if (!(box.x == box.x && box.y == box.y && box.z == box.z && box.w == box.w) ||
+        !(fabsf(box.x) < 1e30f && fabsf(box.y) < 1e30f && fabsf(box.z) < 1e30f && fabsf(box.w) < 1e30f))
+        return all;
+    return box;
+}
+
+__device__ __forceinline__ bool in_box(const float4 b, float px, float py) {
+    return px >= b.x && px <= b.z && py >= b.y && py <= b.w;
 }
 
 // Texture contribution to colour channel k (channels >= 4 have none).

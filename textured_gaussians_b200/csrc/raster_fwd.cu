@@ -1,14 +1,17 @@
 // Textured / plain 2DGS compositor, forward, for sm_100a.
 //
-// One CTA per (camera, tile), one thread per pixel, front-to-back over the
-// tile's depth-sorted splats in batches of blockDim splats staged in shared
-// memory (the gather of each splat's record happens once per CTA, not once
-// per pixel).  Each pixel samples its splat's RGBA texture with one 16-byte
-// (FP32) or 8-byte (BF16/FP16) or 4-byte (FP8) load per bilinear tap and
-// reuses the four taps for the alpha scale and every colour channel.  A warp
-// whose pixels are all saturated stops early; a CTA whose pixels are all
-// saturated stops at the next batch boundary.  Per-Gaussian contribution
-// statistics are reduced across the warp before one global atomic.
+// One CTA per (camera, tile), front-to-back over the tile's depth-sorted
+// splats in batches of tile_size^2 splats staged in shared memory (the gather
+// of each splat's record happens once per CTA, not once per pixel).  Each
+// thread owns PPT pixels of the tile (rows r and r + tile/PPT): the PPT
+// evaluations of a splat are independent, so their texture loads are in flight
+// together, and the splat's shared-memory record is read once for all of them.
+// Each pixel samples its splat's RGBA texture with one 16-byte (FP32), 8-byte
+// (BF16/FP16) or 4-byte (FP8) load per bilinear tap and reuses the four taps for
+// the alpha scale and every colour channel.  A warp whose pixels are all
+// saturated stops early; a CTA whose pixels are all saturated stops at the next
+// batch boundary.  Per-Gaussian contribution statistics are reduced across the
+// warp before one global atomic.
 //
 // Semantics: textured_gaussians/cuda/csrc/rasterize_to_pixels_textured_
 // gaussians_2dgs_fwd.cu:73-445 and rasterize_to_pixels_2dgs_fwd.cu (plain),
@@ -18,12 +21,23 @@
 
 namespace tg {
 
-template <int D, class Tex>
-__global__ void __launch_bounds__(256) raster_fwd_kernel(const tg_raster_fwd_args a) {
+// Resident CTAs per SM the register allocation targets.
+#ifndef TG_FWD_MIN_CTAS
+#define TG_FWD_MIN_CTAS 4
+#endif
+// Pixels per thread for 16x16 tiles.
+#ifndef TG_FWD_PPT
+#define TG_FWD_PPT 1
+#endif
+
+template <int D, class Tex, int PPT>
+__global__ void __launch_bounds__(256 / PPT, TG_FWD_MIN_CTAS) raster_fwd_kernel(const tg_raster_fwd_args a) {
     constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
     extern __shared__ float4 smem4[];
-    const int bs = blockDim.x;
-    float4* s_xyo = smem4;
+    const int nt = blockDim.x;  // threads; the batch holds nt * PPT = tile_size^2 splats
+    const int bs = nt * PPT;
+    float4* s_box = smem4;  // per-splat cull box (see cull_box)
+    float4* s_xyo = s_box + bs;
     float4* s_m0 = s_xyo + bs;
     float4* s_m1 = s_m0 + bs;
     float4* s_m2 = s_m1 + bs;
@@ -31,138 +45,192 @@ __global__ void __launch_bounds__(256) raster_fwd_kernel(const tg_raster_fwd_arg
     float* s_col = reinterpret_cast<float*>(s_nrm + bs);
     int* s_row = reinterpret_cast<int*>(s_col + bs * D);
 
-    const unsigned wmask = __activemask();  // lanes of this warp that exist (tile_size^2 may not fill it)
+    const unsigned wmask = __activemask();
     const TileCoord tc = tile_of_block(a.tile_width, a.tile_height);
     const int tr = threadIdx.x, lane = tr & 31;
     const int ts = a.tile_size;
-    const int i = tc.ty * ts + tr / ts;
-    const int j = tc.tx * ts + tr % ts;
-    const bool inside = i < a.height && j < a.width;
-    const int64_t pix = ((int64_t)tc.c * a.height + i) * a.width + j;
     const int per_cam = a.tile_width * a.tile_height;
 
-    if (a.masks != nullptr && !a.masks[(int64_t)tc.c * per_cam + tc.tile]) {
-        if (inside) {
+    int64_t pix[PPT];
+    bool inside[PPT], done[PPT];
+    float px[PPT], py[PPT];
 #pragma unroll
-            for (int k = 0; k < D; ++k)
-                a.out_colors[pix * D + k] = a.backgrounds ? a.backgrounds[tc.c * D + k] : 0.f;
-            a.out_alphas[pix] = 0.f;
-            a.out_normals[pix * 3] = a.out_normals[pix * 3 + 1] = a.out_normals[pix * 3 + 2] = 0.f;
-            a.out_distort[pix] = 0.f;
-            a.out_median[pix] = 0.f;
-            a.last_ids[pix] = 0;
-            a.median_ids[pix] = 0;
+    for (int q = 0; q < PPT; ++q) {
+        const int local = tr + q * nt;
+        const int i = tc.ty * ts + local / ts;
+        const int j = tc.tx * ts + local % ts;
+        inside[q] = i < a.height && j < a.width;
+        pix[q] = ((int64_t)tc.c * a.height + i) * a.width + j;
+        px[q] = (float)j + 0.5f;
+        py[q] = (float)i + 0.5f;
+        done[q] = !inside[q];
+    }
+
+    if (a.masks != nullptr && !a.masks[(int64_t)tc.c * per_cam + tc.tile]) {
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            if (!inside[q]) continue;
+            const int64_t p = pix[q];
+#pragma unroll
+            for (int k = 0; k < D; ++k) a.out_colors[p * D + k] = a.backgrounds ? a.backgrounds[tc.c * D + k] : 0.f;
+            a.out_alphas[p] = 0.f;
+            a.out_normals[p * 3] = a.out_normals[p * 3 + 1] = a.out_normals[p * 3 + 2] = 0.f;
+            a.out_distort[p] = 0.f;
+            a.out_median[p] = 0.f;
+            a.last_ids[p] = 0;
+            a.median_ids[p] = 0;
         }
         return;
     }
 
+    // pixel-centre rectangle covered by this warp (for the warp-level cull)
+    float wx0 = INFINITY, wx1 = -INFINITY, wy0 = INFINITY, wy1 = -INFINITY;
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+        const int local = tr + q * nt;
+        const float cx = (float)(tc.tx * ts + local % ts) + 0.5f, cy = (float)(tc.ty * ts + local / ts) + 0.5f;
+        wx0 = fminf(wx0, cx); wx1 = fmaxf(wx1, cx); wy0 = fminf(wy0, cy); wy1 = fmaxf(wy1, cy);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        wx0 = fminf(wx0, __shfl_xor_sync(wmask, wx0, o)); wx1 = fmaxf(wx1, __shfl_xor_sync(wmask, wx1, o));
+        wy0 = fminf(wy0, __shfl_xor_sync(wmask, wy0, o)); wy1 = fmaxf(wy1, __shfl_xor_sync(wmask, wy1, o));
+    }
     const int64_t toff = (int64_t)tc.c * per_cam + tc.tile;
     const int32_t range_start = a.tile_offsets[toff];
     const int32_t range_end = (tc.c == a.C - 1 && tc.tile == per_cam - 1) ? (int32_t)a.n_isects : a.tile_offsets[toff + 1];
     const int num_batches = (range_end - range_start + bs - 1) / bs;
-
-    const float px = (float)j + 0.5f, py = (float)i + 0.5f;
     const int64_t tex_stride = (int64_t)a.tex_ry * a.tex_rx;
-    bool done = !inside;
-    float T = 1.f;
-    float pix_out[D];
+
+    float T[PPT], pix_out[PPT][D], nrm_out[PPT][3], distort[PPT], accum_vis_depth[PPT], median_depth[PPT];
+    int32_t cur_idx[PPT], median_idx[PPT];
 #pragma unroll
-    for (int k = 0; k < D; ++k) pix_out[k] = 0.f;
-    float nrm_out[3] = {0.f, 0.f, 0.f};
-    float distort = 0.f, accum_vis_depth = 0.f, median_depth = 0.f;
-    int32_t cur_idx = 0, median_idx = 0;
+    for (int q = 0; q < PPT; ++q) {
+        T[q] = 1.f;
+#pragma unroll
+        for (int k = 0; k < D; ++k) pix_out[q][k] = 0.f;
+        nrm_out[q][0] = nrm_out[q][1] = nrm_out[q][2] = 0.f;
+        distort[q] = accum_vis_depth[q] = median_depth[q] = 0.f;
+        cur_idx[q] = median_idx[q] = 0;
+    }
 
     for (int b = 0; b < num_batches; ++b) {
-        if (__syncthreads_count(done) >= bs) break;
-        const int32_t batch_start = range_start + bs * b;
-        const int32_t idx = batch_start + tr;
-        if (idx < range_end) {
-            const int32_t g = a.flatten_ids[idx];
-            const float2 xy = reinterpret_cast<const float2*>(a.means2d)[g];
-            const int32_t row = a.gaussian_ids ? (int32_t)a.gaussian_ids[g] : g % a.N;
-            const float scale = (Tex::kFormat == TG_TEX_FP8_E4M3) ? a.tex_scales[row] : 1.f;
-            s_xyo[tr] = make_float4(xy.x, xy.y, a.opacities[g], scale);
-            const float* m = a.ray_transforms + 9 * (int64_t)g;
-            s_m0[tr] = make_float4(m[0], m[1], m[2], 0.f);
-            s_m1[tr] = make_float4(m[3], m[4], m[5], 0.f);
-            s_m2[tr] = make_float4(m[6], m[7], m[8], 0.f);
-            const float* n = a.normals + 3 * (int64_t)g;
-            s_nrm[tr] = make_float4(n[0], n[1], n[2], 0.f);
+        bool all_done = true;
 #pragma unroll
-            for (int k = 0; k < D; ++k) s_col[tr * D + k] = a.colors[(int64_t)g * D + k];
-            s_row[tr] = row;
+        for (int q = 0; q < PPT; ++q) all_done &= done[q];
+        if (__syncthreads_count(all_done) >= nt) break;
+        const int32_t batch_start = range_start + bs * b;
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            const int slot = tr + q * nt;
+            const int32_t idx = batch_start + slot;
+            if (idx < range_end) {
+                const int32_t g = a.flatten_ids[idx];
+                const float2 xy = reinterpret_cast<const float2*>(a.means2d)[g];
+                const int32_t row = a.gaussian_ids ? (int32_t)a.gaussian_ids[g] : g % a.N;
+                const float scale = (Tex::kFormat == TG_TEX_FP8_E4M3) ? a.tex_scales[row] : 1.f;
+                s_xyo[slot] = make_float4(xy.x, xy.y, a.opacities[g], scale);
+                const float* m = a.ray_transforms + 9 * (int64_t)g;
+                s_m0[slot] = make_float4(m[0], m[1], m[2], 0.f);
+                s_m1[slot] = make_float4(m[3], m[4], m[5], 0.f);
+                s_m2[slot] = make_float4(m[6], m[7], m[8], 0.f);
+                s_box[slot] = cull_box(s_xyo[slot], s_m0[slot], s_m1[slot], s_m2[slot], kTextured, a.range_x, a.range_y,
+                                       a.g_weight);
+                const float* n = a.normals + 3 * (int64_t)g;
+                s_nrm[slot] = make_float4(n[0], n[1], n[2], 0.f);
+#pragma unroll
+                for (int k = 0; k < D; ++k) s_col[slot * D + k] = a.colors[(int64_t)g * D + k];
+                s_row[slot] = row;
+            }
         }
         __syncthreads();
         const int batch_size = min(bs, range_end - batch_start);
         for (int t = 0; t < batch_size; ++t) {
-            if (__all_sync(wmask, done)) break;
-            bool contributes = false;
-            float alpha = 0.f;
-            if (!done) {
-                PairEval e;
-                const int row = s_row[t];
-                eval_pair<Tex>(e, px, py, s_xyo[t], s_m0[t], s_m1[t], s_m2[t], a.textures, (int64_t)row * tex_stride,
-                               a.tex_rx, a.tex_ry, a.range_x, a.range_y, a.g_weight);
-                if (e.valid) {
-                    const float next_T = T * (1.f - e.alpha);
-                    if (next_T <= 1e-4f) {
-                        done = true;
-                    } else {
-                        const float vis = e.alpha * T;
-                        const float* cp = s_col + t * D;
+            bool warp_done = true;
 #pragma unroll
-                        for (int k = 0; k < D; ++k) pix_out[k] += (cp[k] + (kTextured ? tex_color(e, k) : 0.f)) * vis;
-                        const float4 nn = s_nrm[t];
-                        nrm_out[0] += nn.x * vis;
-                        nrm_out[1] += nn.y * vis;
-                        nrm_out[2] += nn.z * vis;
-                        const float depth = cp[D - 1];
-                        distort += 2.f * (vis * depth * (1.f - T) - vis * accum_vis_depth);
-                        accum_vis_depth += vis * depth;
-                        if (T > 0.5f) {
-                            median_depth = depth;
-                            median_idx = batch_start + t;
-                        }
-                        cur_idx = batch_start + t;
-                        T = next_T;
-                        alpha = e.alpha;
-                        contributes = e.alpha > a.contrib_threshold;
-                    }
+            for (int q = 0; q < PPT; ++q) warp_done &= done[q];
+            if (__all_sync(wmask, warp_done)) break;
+            const float4 box = s_box[t];
+            if (box.z < wx0 || box.x > wx1 || box.w < wy0 || box.y > wy1) continue;  // no pixel of this warp can be valid
+            const float4 xyo = s_xyo[t], m0 = s_m0[t], m1 = s_m1[t], m2 = s_m2[t];
+            const int row = s_row[t];
+            const int64_t tex_base = (int64_t)row * tex_stride;
+            float csum = 0.f;
+            int ccount = 0;
+#pragma unroll
+            for (int q = 0; q < PPT; ++q) {
+                if (done[q] || !in_box(box, px[q], py[q])) continue;
+                PairEval e;
+                eval_pair<Tex>(e, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx, a.tex_ry, a.range_x,
+                               a.range_y, a.g_weight);
+                if (!e.valid) continue;
+                const float next_T = T[q] * (1.f - e.alpha);
+                if (next_T <= 1e-4f) {
+                    done[q] = true;
+                    continue;
+                }
+                const float vis = e.alpha * T[q];
+                const float* cp = s_col + t * D;
+#pragma unroll
+                for (int k = 0; k < D; ++k) pix_out[q][k] += (cp[k] + (kTextured ? tex_color(e, k) : 0.f)) * vis;
+                const float4 nn = s_nrm[t];
+                nrm_out[q][0] += nn.x * vis;
+                nrm_out[q][1] += nn.y * vis;
+                nrm_out[q][2] += nn.z * vis;
+                const float depth = cp[D - 1];
+                distort[q] += 2.f * (vis * depth * (1.f - T[q]) - vis * accum_vis_depth[q]);
+                accum_vis_depth[q] += vis * depth;
+                if (T[q] > 0.5f) {
+                    median_depth[q] = depth;
+                    median_idx[q] = batch_start + t;
+                }
+                cur_idx[q] = batch_start + t;
+                T[q] = next_T;
+                if (e.alpha > a.contrib_threshold) {
+                    csum += e.alpha;
+                    ++ccount;
                 }
             }
-            const unsigned m = __ballot_sync(wmask, contributes);
+            const unsigned m = __ballot_sync(wmask, ccount > 0);
             if (m) {
-                const float s = warp_sum(contributes ? alpha : 0.f, wmask);
+                const float s = warp_sum(csum, wmask);
+                const float c = warp_sum((float)ccount, wmask);
                 if (lane == __ffs(wmask) - 1) {
-                    const int row = s_row[t];
                     atomicAdd(a.contrib_sum + row, s);
-                    atomicAdd(a.contrib_count + row, (float)__popc(m));
+                    atomicAdd(a.contrib_count + row, c);
                 }
             }
         }
     }
-    if (inside) {
-        a.out_alphas[pix] = 1.f - T;
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+        if (!inside[q]) continue;
+        const int64_t p = pix[q];
+        a.out_alphas[p] = 1.f - T[q];
 #pragma unroll
         for (int k = 0; k < D; ++k)
-            a.out_colors[pix * D + k] = a.backgrounds ? pix_out[k] + T * a.backgrounds[tc.c * D + k] : pix_out[k];
-        a.out_normals[pix * 3] = nrm_out[0];
-        a.out_normals[pix * 3 + 1] = nrm_out[1];
-        a.out_normals[pix * 3 + 2] = nrm_out[2];
-        a.last_ids[pix] = cur_idx;
-        a.out_distort[pix] = distort;
-        a.out_median[pix] = median_depth;
-        a.median_ids[pix] = median_idx;
+            a.out_colors[p * D + k] = a.backgrounds ? pix_out[q][k] + T[q] * a.backgrounds[tc.c * D + k] : pix_out[q][k];
+        a.out_normals[p * 3] = nrm_out[q][0];
+        a.out_normals[p * 3 + 1] = nrm_out[q][1];
+        a.out_normals[p * 3 + 2] = nrm_out[q][2];
+        a.last_ids[p] = cur_idx[q];
+        a.out_distort[p] = distort[q];
+        a.out_median[p] = median_depth[q];
+        a.median_ids[p] = median_idx[q];
     }
 }
 
 template <int D, class Tex>
 cudaError_t launch_fwd_t(const tg_raster_fwd_args& a, cudaStream_t s) {
-    const int bs = a.tile_size * a.tile_size;
-    const size_t smem = (size_t)bs * (5 * sizeof(float4) + D * sizeof(float) + sizeof(int));
+    const int tile_px = a.tile_size * a.tile_size;
+    const size_t smem = (size_t)tile_px * (6 * sizeof(float4) + D * sizeof(float) + sizeof(int));
     const int64_t blocks = (int64_t)a.C * a.tile_width * a.tile_height;
     if (blocks == 0) return cudaSuccess;
-    raster_fwd_kernel<D, Tex><<<(unsigned)blocks, bs, smem, s>>>(a);
+    if (tile_px >= 64 * TG_FWD_PPT) {
+        raster_fwd_kernel<D, Tex, TG_FWD_PPT><<<(unsigned)blocks, tile_px / TG_FWD_PPT, smem, s>>>(a);
+    } else {
+        raster_fwd_kernel<D, Tex, 1><<<(unsigned)blocks, tile_px, smem, s>>>(a);
+    }
     note_launches(1);
     return cudaGetLastError();
 }
