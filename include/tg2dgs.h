@@ -100,6 +100,72 @@ typedef struct {
 } tg_project_bwd_args;
 TG_API int tg_project_bwd(const tg_project_bwd_args* a, tg_stream_t stream);
 
+/* ------------------------------------------------------------------ packed projection
+ * Replaces fully_fused_projection_packed_fwd_2dgs_tensor
+ * (textured_gaussians/cuda/csrc/fully_fused_projection_packed_2dgs_fwd.cu:232-324),
+ * split at the one host synchronisation the reference also has (:274-275):
+ * tg_project_packed_count projects every (camera, Gaussian), counts the visible
+ * entries, and writes their total *nnz (device int64) and indptr[C+1]; the
+ * caller reads nnz, allocates the packed outputs and calls
+ * tg_project_packed_emit with the same arguments plus nnz_host and the output
+ * pointers.  Entries are ordered by camera, then Gaussian.  C <= 65535 and
+ * nnz < 2^31 (indptr is int32, as in the reference).  Each camera uses its own
+ * intrinsics Ks[c], as the dense forward and the packed backward do (the
+ * reference's packed forward reads Ks[0] for every camera, :103). */
+typedef struct {
+    int32_t C, N;
+    const float* means;    /* [N,3] */
+    const float* quats;    /* [N,4] */
+    const float* scales;   /* [N,3] */
+    const float* viewmats; /* [C,4,4] */
+    const float* Ks;       /* [C,3,3] */
+    int32_t width, height;
+    float near_plane, far_plane, radius_clip;
+    void* workspace;        /* tg_project_packed_workspace_bytes(C, N) bytes, kept between the two calls */
+    int64_t* nnz;           /* [1] device, written by count */
+    int32_t* indptr;        /* [C+1], written by count */
+    int64_t nnz_host;       /* emit: the value of *nnz */
+    int64_t* camera_ids;    /* [nnz] (emit) */
+    int64_t* gaussian_ids;  /* [nnz] (emit) */
+    int32_t* radii;         /* [nnz] (emit) */
+    float* means2d;         /* [nnz,2] (emit) */
+    float* depths;          /* [nnz] (emit) */
+    float* ray_transforms;  /* [nnz,3,3] (emit) */
+    float* normals;         /* [nnz,3] (emit) */
+} tg_project_packed_args;
+TG_API size_t tg_project_packed_workspace_bytes(int32_t C, int32_t N);
+TG_API int tg_project_packed_count(const tg_project_packed_args* a, tg_stream_t stream);
+TG_API int tg_project_packed_emit(const tg_project_packed_args* a, tg_stream_t stream);
+
+/* Replaces fully_fused_projection_packed_bwd_2dgs_tensor / fully_fused_projection_packed_bwd2_2dgs_tensor
+ * (textured_gaussians/cuda/csrc/fully_fused_projection_packed_2dgs_bwd.cu:172-266, ..._bwd2.cu).
+ * One thread per packed entry; mode as in tg_project_bwd.  sparse_grad = 1:
+ * v_means [nnz,3], v_quats [nnz,4], v_scales [nnz,3] hold each entry's own
+ * gradient (overwritten).  sparse_grad = 0: they are [N,...] and hold the sum
+ * over each Gaussian's entries (zeroed, then accumulated with atomics).
+ * Entries whose camera or Gaussian id is out of range are skipped. */
+typedef struct {
+    int32_t C, N;
+    int64_t nnz;
+    const float* means;
+    const float* quats;
+    const float* scales;
+    const float* viewmats;
+    const float* Ks;
+    const int64_t* camera_ids;     /* [nnz] */
+    const int64_t* gaussian_ids;   /* [nnz] */
+    const float* ray_transforms;   /* [nnz,9] */
+    const float* v_means2d;        /* [nnz,2] */
+    const float* v_depths;         /* [nnz] */
+    const float* v_normals;        /* [nnz,3] */
+    const float* v_ray_transforms; /* [nnz,9] */
+    int32_t mode, sparse_grad;
+    float* v_means;
+    float* v_quats;
+    float* v_scales;
+} tg_project_packed_bwd_args;
+TG_API int tg_project_packed_bwd(const tg_project_packed_bwd_args* a, tg_stream_t stream);
+
 /* ------------------------------------------------------------------ tile intersection
  * Replaces isect_tiles_tensor (textured_gaussians/cuda/csrc/isect_tiles.cu:107-307),
  * split at the one host synchronisation the reference also has (:200-201):

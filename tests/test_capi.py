@@ -69,6 +69,21 @@ def test_invalid_arguments_are_rejected_without_a_device():
     assert L.tg_isect_count(ctypes.byref(ia), None) == -1
     # SH degree above 4
     assert L.tg_sh_fwd(1, 1, 5, 36, None, None, None, None, None) == -1
+    # packed projection: null args, too many cameras, missing workspace, nnz beyond the int32 indptr, bad mode
+    assert L.tg_project_packed_count(None, None) == -1
+    pa = B.ProjectPackedArgs()
+    pa.C, pa.N = 70_000, 10
+    assert L.tg_project_packed_count(ctypes.byref(pa), None) == -2
+    pa.C = 2
+    assert L.tg_project_packed_count(ctypes.byref(pa), None) == -1 and b"workspace" in L.tg_last_error()
+    buf = ctypes.create_string_buffer(256)
+    pa.workspace = pa.nnz = pa.indptr = ctypes.cast(buf, ctypes.c_void_p)
+    pa.N, pa.nnz_host = 0, 1 << 31
+    assert L.tg_project_packed_emit(ctypes.byref(pa), None) == -2
+    pb = B.ProjectPackedBwdArgs()
+    pb.mode = 3
+    assert L.tg_project_packed_bwd(ctypes.byref(pb), None) == -1
+    assert L.tg_project_packed_workspace_bytes(4, 1 << 20) >= 8 * 4 * ((1 << 20) // 4096)
 
 
 def test_product_path_fails_loudly_without_cuda():

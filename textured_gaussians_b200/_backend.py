@@ -38,6 +38,21 @@ class ProjectBwdArgs(ctypes.Structure):
                 ("v_ray_transforms", P), ("mode", I32), ("v_means", P), ("v_quats", P), ("v_scales", P)]
 
 
+class ProjectPackedArgs(ctypes.Structure):
+    _fields_ = [("C", I32), ("N", I32), ("means", P), ("quats", P), ("scales", P), ("viewmats", P), ("Ks", P),
+                ("width", I32), ("height", I32), ("near_plane", F32), ("far_plane", F32), ("radius_clip", F32),
+                ("workspace", P), ("nnz", P), ("indptr", P), ("nnz_host", I64), ("camera_ids", P),
+                ("gaussian_ids", P), ("radii", P), ("means2d", P), ("depths", P), ("ray_transforms", P),
+                ("normals", P)]
+
+
+class ProjectPackedBwdArgs(ctypes.Structure):
+    _fields_ = [("C", I32), ("N", I32), ("nnz", I64), ("means", P), ("quats", P), ("scales", P), ("viewmats", P),
+                ("Ks", P), ("camera_ids", P), ("gaussian_ids", P), ("ray_transforms", P), ("v_means2d", P),
+                ("v_depths", P), ("v_normals", P), ("v_ray_transforms", P), ("mode", I32), ("sparse_grad", I32),
+                ("v_means", P), ("v_quats", P), ("v_scales", P)]
+
+
 class IsectArgs(ctypes.Structure):
     _fields_ = [("n_elems", I64), ("N", I64), ("camera_ids", P), ("means2d", P), ("radii", P), ("depths", P),
                 ("tile_size", I32), ("tile_width", I32), ("tile_height", I32), ("n_cameras", I32),
@@ -85,6 +100,9 @@ def lib() -> ctypes.CDLL:
             for name, argt in [
                 ("tg_project_fwd", [ctypes.POINTER(ProjectFwdArgs), P]),
                 ("tg_project_bwd", [ctypes.POINTER(ProjectBwdArgs), P]),
+                ("tg_project_packed_count", [ctypes.POINTER(ProjectPackedArgs), P]),
+                ("tg_project_packed_emit", [ctypes.POINTER(ProjectPackedArgs), P]),
+                ("tg_project_packed_bwd", [ctypes.POINTER(ProjectPackedBwdArgs), P]),
                 ("tg_isect_count", [ctypes.POINTER(IsectArgs), P]),
                 ("tg_isect_emit", [ctypes.POINTER(IsectArgs), P]),
                 ("tg_sort_pairs", [P, P, P, P, I64, I32, P, ctypes.c_size_t, ctypes.POINTER(I32), P]),
@@ -99,8 +117,9 @@ def lib() -> ctypes.CDLL:
                 fn.restype = ctypes.c_int
             L.tg_kernel_launch_count.restype = ctypes.c_uint64
             L.tg_kernel_launch_count.argtypes = []
-            for name in ("tg_scan_workspace_bytes", "tg_sort_workspace_bytes"):
+            for name in ("tg_scan_workspace_bytes", "tg_sort_workspace_bytes", "tg_project_packed_workspace_bytes"):
                 getattr(L, name).restype = ctypes.c_size_t
+            L.tg_project_packed_workspace_bytes.argtypes = [I32, I32]
             L.tg_scan_workspace_bytes.argtypes = [I64]
             L.tg_sort_workspace_bytes.argtypes = [I64, I32]
             _lib = L

@@ -15,6 +15,10 @@
 namespace tg {
 cudaError_t launch_project_fwd(const tg_project_fwd_args& a, cudaStream_t s);
 cudaError_t launch_project_bwd(const tg_project_bwd_args& a, cudaStream_t s);
+size_t project_packed_workspace_bytes(int32_t C, int32_t N);
+cudaError_t launch_project_packed_count(const tg_project_packed_args& a, cudaStream_t s);
+cudaError_t launch_project_packed_emit(const tg_project_packed_args& a, cudaStream_t s);
+cudaError_t launch_project_packed_bwd(const tg_project_packed_bwd_args& a, cudaStream_t s);
 size_t scan_workspace_bytes(int64_t n_elems);
 cudaError_t launch_isect_count(const tg_isect_args& a, cudaStream_t s);
 cudaError_t launch_isect_emit(const tg_isect_args& a, int tile_n_bits, cudaStream_t s);
@@ -143,6 +147,63 @@ int tg_project_bwd(const tg_project_bwd_args* a, tg_stream_t stream) {
                TG_ERR_INVALID_ARG, "null pointer");
     TG_REQUIRE(aligned(a->quats, 16) && aligned(a->v_quats, 16), TG_ERR_INVALID_ARG, "quats must be 16-byte aligned");
     return cuda_status(tg::launch_project_bwd(*a, stream), "tg_project_bwd");
+}
+
+namespace {
+int check_packed_common(const tg_project_packed_args* a) {
+    TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
+    TG_REQUIRE(a->C >= 0 && a->N >= 0, TG_ERR_INVALID_ARG, "negative sizes");
+    TG_REQUIRE(a->C <= 65535, TG_ERR_UNSUPPORTED, "at most 65535 cameras (got %d)", a->C);
+    TG_REQUIRE(a->workspace && a->nnz && a->indptr, TG_ERR_INVALID_ARG, "null workspace / nnz / indptr");
+    if ((int64_t)a->C * a->N == 0) return TG_OK;
+    TG_REQUIRE(a->means && a->quats && a->scales && a->viewmats && a->Ks, TG_ERR_INVALID_ARG, "null pointer");
+    TG_REQUIRE(aligned(a->quats, 16), TG_ERR_INVALID_ARG, "quats must be 16-byte aligned");
+    return TG_OK;
+}
+}  // namespace
+
+size_t tg_project_packed_workspace_bytes(int32_t C, int32_t N) { return tg::project_packed_workspace_bytes(C, N); }
+
+int tg_project_packed_count(const tg_project_packed_args* a, tg_stream_t stream) {
+    const int rc = check_packed_common(a);
+    if (rc != TG_OK) return rc;
+    return cuda_status(tg::launch_project_packed_count(*a, stream), "tg_project_packed_count");
+}
+
+int tg_project_packed_emit(const tg_project_packed_args* a, tg_stream_t stream) {
+    const int rc = check_packed_common(a);
+    if (rc != TG_OK) return rc;
+    TG_REQUIRE(a->nnz_host >= 0, TG_ERR_INVALID_ARG, "negative nnz");
+    TG_REQUIRE(a->nnz_host < (int64_t(1) << 31), TG_ERR_UNSUPPORTED, "nnz %lld does not fit the int32 indptr",
+               (long long)a->nnz_host);
+    if (a->nnz_host == 0 || (int64_t)a->C * a->N == 0) return TG_OK;
+    TG_REQUIRE(a->camera_ids && a->gaussian_ids && a->radii && a->means2d && a->depths && a->ray_transforms &&
+                   a->normals,
+               TG_ERR_INVALID_ARG, "null output pointer");
+    TG_REQUIRE(aligned(a->means2d, 8), TG_ERR_INVALID_ARG, "means2d must be 8-byte aligned");
+    return cuda_status(tg::launch_project_packed_emit(*a, stream), "tg_project_packed_emit");
+}
+
+int tg_project_packed_bwd(const tg_project_packed_bwd_args* a, tg_stream_t stream) {
+    TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
+    TG_REQUIRE(a->C >= 0 && a->N >= 0 && a->nnz >= 0, TG_ERR_INVALID_ARG, "negative sizes");
+    TG_REQUIRE(a->mode >= 0 && a->mode <= 2, TG_ERR_INVALID_ARG, "bad mode %d", a->mode);
+    TG_REQUIRE(a->nnz < (int64_t(1) << 31), TG_ERR_UNSUPPORTED, "nnz out of range");
+    const int64_t rows = a->sparse_grad ? a->nnz : a->N;
+    if (rows > 0) TG_REQUIRE(a->v_means && a->v_quats && a->v_scales, TG_ERR_INVALID_ARG, "null gradient output");
+    if (rows > 0) TG_REQUIRE(aligned(a->v_quats, 16), TG_ERR_INVALID_ARG, "v_quats must be 16-byte aligned");
+    if (rows > 0) {  // zeroed in both layouts, so skipped entries read as zero
+        cudaError_t e = cudaMemsetAsync(a->v_means, 0, sizeof(float) * 3 * (size_t)rows, stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(a->v_quats, 0, sizeof(float) * 4 * (size_t)rows, stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(a->v_scales, 0, sizeof(float) * 3 * (size_t)rows, stream);
+        if (e != cudaSuccess) return cuda_status(e, "tg_project_packed_bwd");
+    }
+    if (a->nnz == 0) return TG_OK;
+    TG_REQUIRE(a->means && a->quats && a->scales && a->viewmats && a->Ks && a->camera_ids && a->gaussian_ids &&
+                   a->ray_transforms && a->v_means2d && a->v_depths && a->v_normals && a->v_ray_transforms,
+               TG_ERR_INVALID_ARG, "null pointer");
+    TG_REQUIRE(aligned(a->quats, 16), TG_ERR_INVALID_ARG, "quats must be 16-byte aligned");
+    return cuda_status(tg::launch_project_packed_bwd(*a, stream), "tg_project_packed_bwd");
 }
 
 size_t tg_scan_workspace_bytes(int64_t n_elems) { return tg::scan_workspace_bytes(n_elems); }

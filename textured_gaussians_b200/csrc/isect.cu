@@ -14,7 +14,7 @@
 // global digit offsets by decoupled look-back over earlier tiles.  Every
 // look-back wait is bounded; a wait that gives up raises a workspace error
 // flag that the host turns into TG_ERR_TIMEOUT.
-#include "tg_common.cuh"
+#include "scan.cuh"
 
 namespace tg {
 
@@ -29,38 +29,6 @@ __device__ __forceinline__ void tile_box(float mx, float my, int32_t radius, int
     y0 = min((uint32_t)floorf(ty - tr), th);
     x1 = min((uint32_t)ceilf(tx + tr), tw);
     y1 = min((uint32_t)ceilf(ty + tr), th);
-}
-
-constexpr int kScanThreads = 256;
-constexpr int kScanItems = 16;
-constexpr int kScanChunk = kScanThreads * kScanItems;
-
-__device__ __forceinline__ int64_t warp_incl_scan(int64_t v) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int64_t u = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += u;
-    }
-    return v;
-}
-
-// Block-wide exclusive scan of one int64 per thread (blockDim = kScanThreads).
-__device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t* s_warp, int64_t& total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t inc = warp_incl_scan(v);
-    if (lane == 31) s_warp[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        int64_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0;
-        w = warp_incl_scan(w);
-        if (lane < kScanThreads / 32) s_warp[lane] = w;
-    }
-    __syncthreads();
-    const int64_t warp_prefix = warp == 0 ? 0 : s_warp[warp - 1];
-    total = s_warp[kScanThreads / 32 - 1];
-    __syncthreads();
-    return warp_prefix + inc - v;
 }
 
 // Phase 1: tile counts per element and per-chunk sums.
@@ -102,6 +70,12 @@ __global__ void __launch_bounds__(kScanThreads) scan_chunk_sums_kernel(int64_t* 
         carry += total;
     }
     if (threadIdx.x == 0) *n_total = carry;
+}
+
+cudaError_t launch_scan_chunk_sums(int64_t* chunk_sums, int64_t n_chunks, int64_t* n_total, cudaStream_t s) {
+    scan_chunk_sums_kernel<<<1, kScanThreads, 0, s>>>(chunk_sums, n_chunks, n_total);
+    note_launches(1);
+    return cudaGetLastError();
 }
 
 // Phase 3: inclusive prefix of tiles_per_gauss within each chunk plus the chunk offset.
@@ -188,7 +162,6 @@ struct SortWorkspace {
     size_t bytes;
 };
 
-__host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 inline SortWorkspace carve_sort_workspace(void* base, int64_t n, int passes) {
     SortWorkspace w;

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "../../include/tg2dgs.h"
 
 namespace tg {
@@ -14,6 +16,8 @@ constexpr int kNumSMs = 148;  // B200: 2 dies x 74 SMs
 
 // Process-wide count of kernel launches (defined in capi.cu).
 void note_launches(unsigned n);
+
+__host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct f3 {
     float x, y, z;

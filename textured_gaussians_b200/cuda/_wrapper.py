@@ -142,8 +142,13 @@ def fully_fused_projection_2dgs(
     (reference: cuda/_wrapper.py:1267-1371).
 
     Returns ``(radii, means2d, depths, ray_transforms, normals)`` for the dense
-    layout.  ``adjoint="exact"`` selects the exact derivative of means2d with
-    respect to the ray transform in the backward (the reference keeps only its
+    layout and ``(camera_ids, gaussian_ids, radii, means2d, depths,
+    ray_transforms, normals)`` for the packed one (visible entries only,
+    ordered by camera then Gaussian; reference: cuda/_wrapper.py:1487-1644).
+    With ``sparse_grad`` the packed backward returns the gradients of means,
+    quats and scales as sparse COO tensors with one row per entry.
+    ``adjoint="exact"`` selects the exact derivative of means2d with respect
+    to the ray transform in the backward (the reference keeps only its
     diagonal terms).
     """
     C = viewmats.size(0)
@@ -157,9 +162,11 @@ def fully_fused_projection_2dgs(
     assert scales.size() == (N, 3), scales.size()
     if sparse_grad:
         assert packed, "sparse_grad is only supported when packed is True"
-    if packed:
-        raise NotImplementedError("packed=True projection is not available in this build")
     mode = B.TG_ADJ_EXACT if adjoint == "exact" else (B.TG_ADJ_BWD2 if norm_rot_grad else B.TG_ADJ_REFERENCE)
+    if packed:
+        return _FullyFusedProjectionPacked2DGS.apply(
+            means.contiguous(), quats.contiguous(), scales.contiguous(), viewmats.contiguous(), Ks.contiguous(),
+            width, height, eps2d, near_plane, far_plane, radius_clip, sparse_grad, mode)
     return _FullyFusedProjection2DGS.apply(
         means.contiguous(), quats.contiguous(), scales.contiguous(), viewmats.contiguous(), Ks.contiguous(),
         width, height, eps2d, near_plane, far_plane, radius_clip, mode)
@@ -215,6 +222,85 @@ class _FullyFusedProjection2DGS(torch.autograd.Function):
         return (v_means if ctx.needs_input_grad[0] else None, v_quats if ctx.needs_input_grad[1] else None,
                 v_scales if ctx.needs_input_grad[2] else None, v_viewmats,
                 None, None, None, None, None, None, None, None)
+
+
+class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
+    """Packed projection (reference: cuda/_wrapper.py:1487-1644).
+
+    Two passes split at one host read of nnz, as in the reference.  Every
+    camera uses its own intrinsics (the reference's packed forward reads
+    Ks[0] for all cameras).
+    """
+
+    @staticmethod
+    def forward(ctx, means, quats, scales, viewmats, Ks, width, height, eps2d, near_plane, far_plane, radius_clip,
+                sparse_grad, mode):
+        C, N = viewmats.shape[0], means.shape[0]
+        dev = means.device
+        ws = torch.empty((B.lib().tg_project_packed_workspace_bytes(C, N),), dtype=torch.uint8, device=dev)
+        nnz_dev = torch.empty((1,), dtype=torch.int64, device=dev)
+        indptr = torch.empty((C + 1,), dtype=torch.int32, device=dev)
+        a = B.ProjectPackedArgs(C, N, B.ptr(means), B.ptr(quats), B.ptr(scales), B.ptr(viewmats), B.ptr(Ks),
+                                int(width), int(height), float(near_plane), float(far_plane), float(radius_clip),
+                                B.ptr(ws), B.ptr(nnz_dev), B.ptr(indptr), 0)
+        st = B.stream_of(means)
+        B.call("tg_project_packed_count", st, B.lib().tg_project_packed_count, ctypes.byref(a), st)
+        nnz = int(nnz_dev.item())  # the one host synchronisation, as in the reference
+        camera_ids = torch.empty((nnz,), dtype=torch.int64, device=dev)
+        gaussian_ids = torch.empty((nnz,), dtype=torch.int64, device=dev)
+        radii = torch.empty((nnz,), dtype=torch.int32, device=dev)
+        means2d = torch.empty((nnz, 2), dtype=torch.float32, device=dev)
+        depths = torch.empty((nnz,), dtype=torch.float32, device=dev)
+        ray_transforms = torch.empty((nnz, 3, 3), dtype=torch.float32, device=dev)
+        normals = torch.empty((nnz, 3), dtype=torch.float32, device=dev)
+        a.nnz_host = nnz
+        a.camera_ids, a.gaussian_ids, a.radii = B.ptr(camera_ids), B.ptr(gaussian_ids), B.ptr(radii)
+        a.means2d, a.depths, a.ray_transforms, a.normals = (B.ptr(means2d), B.ptr(depths), B.ptr(ray_transforms),
+                                                            B.ptr(normals))
+        B.call("tg_project_packed_emit", st, B.lib().tg_project_packed_emit, ctypes.byref(a), st)
+        ctx.save_for_backward(camera_ids, gaussian_ids, means, quats, scales, viewmats, Ks, ray_transforms)
+        ctx.sparse_grad = bool(sparse_grad)
+        ctx.mode = mode
+        ctx.mark_non_differentiable(camera_ids, gaussian_ids, radii)
+        return camera_ids, gaussian_ids, radii, means2d, depths, ray_transforms, normals
+
+    @staticmethod
+    def backward(ctx, v_camera_ids, v_gaussian_ids, v_radii, v_means2d, v_depths, v_ray_transforms, v_normals):
+        camera_ids, gaussian_ids, means, quats, scales, viewmats, Ks, ray_transforms = ctx.saved_tensors
+        C, N, nnz = viewmats.shape[0], means.shape[0], camera_ids.shape[0]
+        dev = means.device
+
+        def z(t, shape):
+            return torch.zeros(shape, dtype=torch.float32, device=dev) if t is None else t.float().contiguous()
+
+        v_means2d = z(v_means2d, (nnz, 2))
+        v_depths = z(v_depths, (nnz,))
+        v_ray_transforms = z(v_ray_transforms, (nnz, 3, 3))
+        v_normals = z(v_normals, (nnz, 3))
+        rows = nnz if ctx.sparse_grad else N
+        v_means = torch.empty((rows, 3), dtype=torch.float32, device=dev)
+        v_quats = torch.empty((rows, 4), dtype=torch.float32, device=dev)
+        v_scales = torch.empty((rows, 3), dtype=torch.float32, device=dev)
+        a = B.ProjectPackedBwdArgs(C, N, nnz, B.ptr(means), B.ptr(quats), B.ptr(scales), B.ptr(viewmats), B.ptr(Ks),
+                                   B.ptr(camera_ids), B.ptr(gaussian_ids), B.ptr(ray_transforms), B.ptr(v_means2d),
+                                   B.ptr(v_depths), B.ptr(v_normals), B.ptr(v_ray_transforms), ctx.mode,
+                                   int(ctx.sparse_grad), B.ptr(v_means), B.ptr(v_quats), B.ptr(v_scales))
+        st = B.stream_of(means)
+        B.call("tg_project_packed_bwd", st, B.lib().tg_project_packed_bwd, ctypes.byref(a), st)
+
+        def out(v, like, need):
+            if not need:
+                return None
+            if ctx.sparse_grad:
+                return torch.sparse_coo_tensor(indices=gaussian_ids[None], values=v, size=like.size(),
+                                               is_coalesced=len(viewmats) == 1)
+            return v
+
+        # the reference gates the (never written, zero) viewmats gradient on the Ks input (index 4)
+        v_viewmats = torch.zeros_like(viewmats) if ctx.needs_input_grad[4] else None
+        return (out(v_means, means, ctx.needs_input_grad[0]), out(v_quats, quats, ctx.needs_input_grad[1]),
+                out(v_scales, scales, ctx.needs_input_grad[2]), v_viewmats,
+                None, None, None, None, None, None, None, None, None)
 
 
 # --------------------------------------------------------------------------- intersection
@@ -386,18 +472,16 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
     @staticmethod
     def forward(ctx, means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, masks,
                 tex_store, tex_scales, range_x, range_y, width, height, tile_size, isect_offsets, flatten_ids,
-                absgrad, gs_contrib_threshold, g_weight, adjoint, bg_grad_index_ok):
+                absgrad, gs_contrib_threshold, g_weight, adjoint, bg_grad_index_ok, gaussian_ids, n_rows):
         dev = means2d.device
-        packed = means2d.dim() == 2
         C = isect_offsets.shape[0]
-        if packed:
-            raise NotImplementedError("packed rasterization is not available in this build")
-        N = means2d.shape[1]
-        n_contrib = N
+        # N: row modulus of the dense layout, or the packed entry count (row = entry) without gaussian_ids
+        N = means2d.shape[1] if means2d.dim() == 3 else means2d.shape[0]
+        n_contrib = N if gaussian_ids is None else n_rows
         D = colors.shape[-1]
         m = None if masks is None else masks.to(torch.uint8).contiguous()
         a = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
-                      backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, None, n_contrib,
+                      backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
                       gs_contrib_threshold, g_weight, C, N)
         render_colors = torch.empty((C, height, width, D), dtype=torch.float32, device=dev)
         render_alphas = torch.empty((C, height, width, 1), dtype=torch.float32, device=dev)
@@ -416,9 +500,9 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         B.call("tg_rasterize_fwd", st, B.lib().tg_rasterize_fwd, ctypes.byref(a), st)
         ctx.save_for_backward(means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, m,
                               tex_store, tex_scales, isect_offsets, flatten_ids, render_colors, render_alphas,
-                              last_ids, median_ids)
+                              last_ids, median_ids, gaussian_ids)
         ctx.cfg = (range_x, range_y, width, height, tile_size, absgrad, g_weight, adjoint, bg_grad_index_ok,
-                   gs_contrib_threshold)
+                   gs_contrib_threshold, N, n_contrib)
         ctx.mark_non_differentiable(contrib_sum, contrib_count)
         return render_colors, render_alphas, render_normals, render_distort, render_median, contrib_sum, contrib_count
 
@@ -426,11 +510,12 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
     def backward(ctx, v_render_colors, v_render_alphas, v_render_normals, v_render_distort, v_render_median,
                  v_contrib_sum, v_contrib_count):
         (means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, m, tex_store, tex_scales,
-         isect_offsets, flatten_ids, render_colors, render_alphas, last_ids, median_ids) = ctx.saved_tensors
+         isect_offsets, flatten_ids, render_colors, render_alphas, last_ids, median_ids,
+         gaussian_ids) = ctx.saved_tensors
         (range_x, range_y, width, height, tile_size, absgrad, g_weight, adjoint, bg_grad_index_ok,
-         gs_contrib_threshold) = ctx.cfg
+         gs_contrib_threshold, N, n_contrib) = ctx.cfg
         dev = means2d.device
-        C, N = isect_offsets.shape[0], means2d.shape[1]
+        C = isect_offsets.shape[0]
         D = colors.shape[-1]
 
         def g(t, shape):
@@ -442,8 +527,8 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         v_rd = g(v_render_distort, (C, height, width, 1))
         v_rm = g(v_render_median, (C, height, width, 1))
         f = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
-                      backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, None, N, 0.0, g_weight,
-                      C, N)
+                      backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
+                      0.0, g_weight, C, N)
         v_means2d = torch.empty_like(means2d)
         v_means2d_abs = torch.empty_like(means2d) if absgrad else None
         v_ray_transforms = torch.empty_like(ray_transforms)
@@ -455,7 +540,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         v_densify = torch.empty_like(densify)
         a = B.RasterBwdArgs(f, B.ptr(render_colors), B.ptr(render_alphas), B.ptr(last_ids), B.ptr(median_ids),
                             B.ptr(v_rc), B.ptr(v_ra), B.ptr(v_rn), B.ptr(v_rd), B.ptr(v_rm), int(adjoint),
-                            means2d.shape[0] * means2d.shape[1], B.ptr(v_means2d), B.ptr(v_means2d_abs),
+                            means2d.numel() // 2, B.ptr(v_means2d), B.ptr(v_means2d_abs),
                             B.ptr(v_ray_transforms), B.ptr(v_colors), B.ptr(v_opacities), B.ptr(v_normals),
                             B.ptr(v_textures), B.ptr(v_densify))
         st = B.stream_of(means2d)
@@ -468,7 +553,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         if v_textures is not None and textures.dtype != torch.float32:
             v_textures = v_textures.to(textures.dtype)
         return (v_means2d, v_ray_transforms, v_colors, v_opacities, v_textures, v_normals, v_densify, v_backgrounds,
-                None, None, None, None, None, None, None, None, None, None, None, None, None, None, None)
+                None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None)
 
 
 def _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
@@ -519,6 +604,7 @@ def rasterize_to_pixels_textured_gaussians(
     *,
     texture_storage: Optional[Tensor] = None,
     texture_scales: Optional[Tensor] = None,
+    gaussian_ids: Optional[Tensor] = None,
 ) -> Tuple[Tensor, ...]:
     """Rasterize textured 2D Gaussians to pixels (reference: cuda/_wrapper.py:1806-2002).
 
@@ -527,12 +613,25 @@ def rasterize_to_pixels_textured_gaussians(
     gs_contrib_count)``.  ``texture_storage`` (BF16 / FP16 / FP8-E4M3, same
     [N, th, tw, 4] layout, plus ``texture_scales`` [N] for FP8) is sampled in
     place of ``textures``; gradients still flow to ``textures`` in FP32.
+
+    Packed inputs ([nnz, ...]) need ``gaussian_ids`` [nnz] (the packed
+    projection's output): entry e samples texture row ``gaussian_ids[e]`` and
+    the contribution statistics are per Gaussian, [N].  The reference indexes
+    textures and statistics with the packed entry index, out of range for
+    packed inputs, so it is not followed there.
     """
     _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
                   backgrounds, packed)
     if filtering not in _FILTER_ADJOINT:
         raise Exception(f"Unsupported filter type {filtering}")
     assert textures.dim() == 4 and textures.shape[-1] == 4, textures.shape
+    if packed:
+        if gaussian_ids is None:
+            raise ValueError("packed textured rasterization needs gaussian_ids (texture row of each packed entry)")
+        assert gaussian_ids.shape == (means2d.shape[0],), gaussian_ids.shape
+        gaussian_ids = gaussian_ids.to(torch.int64).contiguous()
+    else:
+        gaussian_ids = None
     colors, backgrounds, padded = _pad_channels(colors, backgrounds)
     store = textures if texture_storage is None else texture_storage
     store = store.contiguous()
@@ -547,7 +646,7 @@ def rasterize_to_pixels_textured_gaussians(
         None if backgrounds is None else backgrounds.contiguous(), masks, store, texture_scales,
         float(texture_range_x), float(texture_range_y), int(image_width), int(image_height), int(tile_size),
         isect_offsets.contiguous(), flatten_ids.contiguous(), absgrad, gs_contrib_threshold, g_weight,
-        _FILTER_ADJOINT[filtering], False)
+        _FILTER_ADJOINT[filtering], False, gaussian_ids, textures.shape[0])
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]
@@ -572,21 +671,35 @@ def rasterize_to_pixels_2dgs(
     absgrad: bool = False,
     distloss: bool = False,
     gs_contrib_threshold: float = 0.0,
+    *,
+    gaussian_ids: Optional[Tensor] = None,
+    n_gaussians: Optional[int] = None,
 ) -> Tuple[Tensor, ...]:
     """Rasterize plain 2D Gaussians to pixels (reference: cuda/_wrapper.py:1647-1784).
 
     Same 7-tuple as the textured form; the background gradient is computed
     when the backgrounds require it (reference: cuda/_wrapper.py:2920-2925).
+    Packed inputs: the contribution statistics are per entry, [nnz], or per
+    Gaussian, [n_gaussians], when ``gaussian_ids`` and ``n_gaussians`` are
+    given (the reference sizes them [0] for packed inputs).
     """
     _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
                   backgrounds, packed)
+    if packed and gaussian_ids is not None:
+        if n_gaussians is None:
+            raise ValueError("gaussian_ids needs n_gaussians")
+        assert gaussian_ids.shape == (means2d.shape[0],), gaussian_ids.shape
+        gaussian_ids = gaussian_ids.to(torch.int64).contiguous()
+    else:
+        gaussian_ids, n_gaussians = None, 0
     colors, backgrounds, padded = _pad_channels(colors, backgrounds)
     dummy = torch.empty((0, 1, 1, 4), dtype=torch.float32, device=means2d.device)
     out = _RasterizeToPixelsTextured.apply(
         means2d.contiguous(), ray_transforms.contiguous(), colors.contiguous().float(), opacities.contiguous(), dummy,
         normals.contiguous(), densify.contiguous(), None if backgrounds is None else backgrounds.contiguous(), masks,
         None, None, 3.0, 3.0, int(image_width), int(image_height), int(tile_size), isect_offsets.contiguous(),
-        flatten_ids.contiguous(), absgrad, gs_contrib_threshold, 1.0, B.TG_ADJ_REFERENCE, True)
+        flatten_ids.contiguous(), absgrad, gs_contrib_threshold, 1.0, B.TG_ADJ_REFERENCE, True, gaussian_ids,
+        int(n_gaussians))
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]

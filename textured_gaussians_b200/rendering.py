@@ -8,6 +8,10 @@ Every stage runs this package's sm_100a kernels; the glue between them
 (repeat of opacities, camera centres, clamps, ED division, normal rotation)
 is torch on the same device.
 
+``packed=True`` runs the packed layout end to end (visible (camera, Gaussian)
+entries only, ``meta["camera_ids"]`` / ``meta["gaussian_ids"]``), with
+``sparse_grad`` giving COO gradients for means, quats and scales.
+
 Extensions (keyword-only, default off): ``texture_storage`` /
 ``texture_scales`` (sample BF16 / FP16 / FP8 textures, gradients to the FP32
 ``textures``), ``filtering="bilinear_exact"`` and ``adjoint="exact"`` (exact
@@ -57,11 +61,16 @@ def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, heigh
         assert colors.dim() == 3 and colors.shape[0] == N and colors.shape[2] == 3, colors.shape
         assert (sh_degree + 1) ** 2 <= colors.shape[1], colors.shape
 
-    radii, means2d, depths, ray_transforms, normals = fully_fused_projection_2dgs(
+    proj = fully_fused_projection_2dgs(
         means, quats, scales, viewmats, Ks, width, height, eps2d, near_plane, far_plane, radius_clip, packed,
         sparse_grad, norm_rot_grad, adjoint=adjoint)
-    opacities = opacities.repeat(C, 1)
-    camera_ids, gaussian_ids = None, None
+    if packed:
+        camera_ids, gaussian_ids, radii, means2d, depths, ray_transforms, normals = proj
+        opacities = opacities[gaussian_ids]
+    else:
+        radii, means2d, depths, ray_transforms, normals = proj
+        opacities = opacities.repeat(C, 1)
+        camera_ids, gaussian_ids = None, None
 
     densify = torch.zeros_like(means2d, dtype=means.dtype, requires_grad=True, device=means.device)
     tile_width = math.ceil(width / float(tile_size))
@@ -73,11 +82,17 @@ def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, heigh
 
     if sh_degree is not None:
         camtoworlds = torch.inverse(viewmats)
-        dirs = means[None, :, :] - camtoworlds[:, None, :3, 3]
-        colors = spherical_harmonics_shared(sh_degree, dirs, colors, masks=radii > 0)  # [C, N, 3]
+        if packed:
+            dirs = means[gaussian_ids, :] - camtoworlds[camera_ids, :3, 3]
+            colors = spherical_harmonics(sh_degree, dirs, colors[gaussian_ids], masks=radii > 0)  # [nnz, 3]
+        else:
+            dirs = means[None, :, :] - camtoworlds[:, None, :3, 3]
+            colors = spherical_harmonics_shared(sh_degree, dirs, colors, masks=radii > 0)  # [C, N, 3]
         colors = torch.clamp_min(colors + 0.5, 0.0)
     elif colors.dim() == 2:
-        colors = colors.expand(C, *([-1] * colors.dim()))
+        colors = colors[gaussian_ids] if packed else colors.expand(C, *([-1] * colors.dim()))
+    elif packed:
+        colors = colors[camera_ids, gaussian_ids, :]
 
     if render_mode in ["RGB+D", "RGB+ED"]:
         colors = torch.cat((colors, depths[..., None]), dim=-1)
@@ -166,7 +181,8 @@ def rasterization_2dgs(
     outs = rasterize_to_pixels_2dgs(
         p["means2d"], p["ray_transforms"], p["colors"], p["opacities"], p["normals"], p["densify"], width, height,
         tile_size, p["isect_offsets"], p["flatten_ids"], backgrounds=backgrounds, packed=packed, absgrad=absgrad,
-        distloss=distloss, gs_contrib_threshold=gs_contrib_threshold)
+        distloss=distloss, gs_contrib_threshold=gs_contrib_threshold, gaussian_ids=p["gaussian_ids"],
+        n_gaussians=means.shape[0] if packed else None)
     return _finish(p, *outs, viewmats, Ks, width, height, tile_size, render_mode, depth_mode)
 
 
@@ -221,5 +237,5 @@ def rasterization_textured_gaussians(
         p["normals"], p["densify"], width, height, tile_size, p["isect_offsets"], p["flatten_ids"],
         backgrounds=backgrounds, packed=packed, absgrad=absgrad, distloss=distloss,
         gs_contrib_threshold=gs_contrib_threshold, filtering=filtering, g_weight=g_weight,
-        texture_storage=texture_storage, texture_scales=texture_scales)
+        texture_storage=texture_storage, texture_scales=texture_scales, gaussian_ids=p["gaussian_ids"])
     return _finish(p, *outs, viewmats, Ks, width, height, tile_size, render_mode, depth_mode)
