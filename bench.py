@@ -232,7 +232,8 @@ def _run_ours(args, rank, world, local, dev):
         for v in views:  # the plain drop-in renders one camera per call, as the reference must (C > 1 misindexes)
             out = rasterization_textured_gaussians(means, quats, scales, opac, colors, tex32, viewmats[v], Ks[v], W, H,
                                                    sh_degree=0, far_plane=100.0, tile_size=tile_size,
-                                                   texture_storage=storage)
+                                                   texture_storage=storage,
+                                                   tile_order=args.tile_order)
             loss = (out[0] * w_rgb[v]).sum() + (out[1] * w_a[v]).sum()
             loss.backward()
         return out, loss
@@ -312,6 +313,7 @@ def _run_ours(args, rank, world, local, dev):
                                f"(FP32 master + FP32 gradients), {C} cameras 1600x1200 per GPU in one call, "
                                f"tile {tile} (autotuned), fwd+bwd",
                    "texture_storage": "bf16", "tile_size": tile, "tile_tuning_ms": tune_ms, "splats": N,
+                   "tile_order": args.tile_order,
                    "cameras_per_gpu": C, "width": W, "height": H,
                    "l2": "inputs larger than L2 (BF16 textures 8.4 GB, FP32 master 16.8 GB)",
                    "parallelism": f"replicas x{world}"},
@@ -428,6 +430,159 @@ def cpu_baseline(args, sample_tiles: int = 16):
                       f"({frac * 100:.1f}% of pixels, {t_raster:.2f} s); FP32 oracle, OpenMP"}
 
 
+# ---------------------------------------------------------------- batching form (64 uneven views, 3 scenes)
+BATCH_SIZES = [(400, 300), (800, 600), (1297, 840), (1600, 1200)]
+
+
+def make_batch_workload(n_views=64, scene_sizes=(200_000, 500_000, 1_000_000), seed=4):
+    """Three mixture scenes (as the 1M workload, seeds 4, 5, 6), 64 views with resolutions drawn uniformly from
+    BATCH_SIZES (fx = fy = W, principal point at the centre), view c showing scene c % 3 from the
+    (c // 3)-th of that scene's radius-25 Fibonacci directions."""
+    from textured_gaussians_b200 import scenes
+
+    parts = []
+    for s, n in enumerate(scene_sizes):
+        sc = make_scene_seeded(n, seed + s)
+        parts.append(sc)
+    rng = np.random.default_rng(seed)
+    sizes = [BATCH_SIZES[i] for i in rng.integers(0, len(BATCH_SIZES), size=n_views)]
+    view_scenes = [c % len(scene_sizes) for c in range(n_views)]
+    per_scene = [sum(1 for v in view_scenes if v == s) for s in range(len(scene_sizes))]
+    dirs = [scenes.fibonacci_dirs(k) for k in per_scene]
+    V = np.stack([scenes.look_at(25.0 * dirs[view_scenes[c]][c // len(scene_sizes)]) for c in range(n_views)])
+    K = np.stack([scenes.intrinsics(w, w / 2, h / 2) for w, h in sizes])
+    cat = {k: np.concatenate([p[k] for p in parts]) for k in ("means", "quats", "scales", "opacities", "colors")}
+    offs = np.cumsum([0] + list(scene_sizes)).tolist()
+    return cat, offs, V.astype(np.float32), K.astype(np.float32), sizes, view_scenes
+
+
+def make_scene_seeded(n_splats: int, seed: int):
+    """The mixture scene of make_scene with its own seed (Gaussians only)."""
+    rng = np.random.default_rng(seed)
+    n_comp = 64
+    u = rng.normal(size=(n_comp, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    centres = u * (10.0 * rng.uniform(0, 1, size=(n_comp, 1)) ** (1.0 / 3.0))
+    comp = rng.integers(0, n_comp, size=n_splats)
+    means = centres[comp] + rng.normal(0, 0.5, size=(n_splats, 3))
+    ls = rng.normal(-3.5, 0.6, size=(n_splats, 2))
+    scales = np.exp(np.concatenate([ls, ls[:, 1:2]], 1))
+    q = rng.normal(size=(n_splats, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    opac = 1.0 / (1.0 + np.exp(-rng.normal(0.5, 1.0, size=n_splats)))
+    colors = rng.uniform(0, 1, size=(n_splats, 1, 3))
+    f32 = lambda x: x.astype(np.float32)
+    return dict(means=f32(means), quats=f32(q), scales=f32(scales), opacities=f32(opac), colors=f32(colors))
+
+
+def run_batch(args):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    with torch.cuda.stream(torch.cuda.Stream(dev)):
+        _run_batch(args, dev)
+
+
+def _run_batch(args, dev):
+    """Config of the batching form: one call renders all 64 views (BF16 texture storage, heaviest tiles first,
+    tile autotuned) against the FP32 plain drop-in called once per view at tile 16."""
+    import torch
+    from textured_gaussians_b200 import _backend as B
+    from textured_gaussians_b200 import rasterization_textured_gaussians
+    from textured_gaussians_b200.batch import ViewTable, rasterization_textured_gaussians_batch
+    from textured_gaussians_b200.cuda import make_texture_storage
+    from textured_gaussians_b200.tuning import autotune_tile_size
+
+    cat, offs, V, K, sizes, vs = make_batch_workload(n_views=args.views)
+    T = lambda x: torch.from_numpy(x).to(dev)
+    L = {k: T(v).requires_grad_() for k, v in cat.items()}
+    R = args.tex
+    N = offs[-1]
+    tex32 = torch.cat([gpu_textures(offs[s + 1] - offs[s], R, dev, seed=4 + s) for s in range(len(offs) - 1)])
+    tex32.requires_grad_()
+    store, _ = make_texture_storage(tex32.detach(), "bf16")
+    viewmats, Ks = T(V), T(K)
+    widths, heights = [w for w, _ in sizes], [h for _, h in sizes]
+    n_pix = sum(w * h for w, h in sizes)
+    g = torch.Generator(device=dev)
+    g.manual_seed(11)
+    w_flat = torch.randn((n_pix, 4), generator=g, device=dev)
+    pix_base = np.cumsum([0] + [w * h for w, h in sizes]).tolist()
+    tables = {}
+
+    def zero():
+        for t in list(L.values()) + [tex32]:
+            t.grad = None
+
+    def step_batch(tile, order):
+        zero()
+        vt = tables.get(tile)
+        if vt is None:
+            vt = tables[tile] = ViewTable(widths, heights, tile, dev)
+        out = rasterization_textured_gaussians_batch(
+            L["means"], L["quats"], L["scales"], L["opacities"], L["colors"], tex32, offs, viewmats, Ks, widths,
+            heights, vs, sh_degree=0, far_plane=100.0, tile_size=tile, texture_storage=store, tile_order=order,
+            view_table=vt)
+        meta = out[-1]
+        loss = (meta["flat_colors"] * w_flat[:, :3]).sum() + (meta["flat_alphas"] * w_flat[:, 3:]).sum()
+        loss.backward()
+        return meta
+
+    def step_per_view():
+        zero()
+        for c, (w, h) in enumerate(sizes):
+            a, b = offs[vs[c]], offs[vs[c] + 1]
+            out = rasterization_textured_gaussians(
+                L["means"][a:b], L["quats"][a:b], L["scales"][a:b], L["opacities"][a:b], L["colors"][a:b],
+                tex32[a:b], viewmats[c:c + 1], Ks[c:c + 1], w, h, sh_degree=0, far_plane=100.0, tile_size=16)
+            wv = w_flat[pix_base[c]:pix_base[c + 1]]
+            loss = (out[0].reshape(-1, 3) * wv[:, :3]).sum() + (out[1].reshape(-1, 1) * wv[:, 3:]).sum()
+            loss.backward()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        l0 = B.lib().tg_kernel_launch_count()
+        B.TIMERS.enable(True)
+        t0.record()
+        for _ in range(steps):
+            fn()
+        t1.record()
+        torch.cuda.synchronize()
+        stages = {k: round(statistics.mean(v), 3) for k, v in B.TIMERS.summary().items()}
+        B.TIMERS.enable(False)
+        return t0.elapsed_time(t1) / steps, stages, B.lib().tg_kernel_launch_count() - l0
+
+    tile, tune_ms = autotune_tile_size(("batch", N, len(sizes)), lambda ts: step_batch(ts, "heaviest_first"),
+                                       repeats=1)
+    with ClockSampler(0) as clk:
+        ms_b, stages_b, launches_b = timed(lambda: step_batch(tile, "heaviest_first"), args.steps, args.warmup)
+    ms_launch, _, _ = timed(lambda: step_batch(tile, "launch"), args.steps, 1)
+    ms_pv, stages_pv, launches_pv = timed(step_per_view, args.steps, 1)
+    line = {
+        "metric": "textured 2DGS fwd+bwd Mpix/s, batching form: 64 uneven views over 3 scenes in one call",
+        "value": round(n_pix / (ms_b / 1e3) / 1e6, 2), "unit": "Mpix/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_b, 3), "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"3 mixture scenes N=200k/500k/1M ({N:,} splats), {R}x{R} RGBA textures in BF16 "
+                               f"storage, {len(sizes)} views drawn from {BATCH_SIZES}, {n_pix:,} pixels, "
+                               f"tile {tile} (autotuned), heaviest tiles first, fwd+bwd",
+                   "tile_tuning_ms": tune_ms, "views": len(sizes), "pixels": n_pix, "splats": N},
+        "splats_per_s": round(sum(offs[s + 1] - offs[s] for s in vs) / (ms_b / 1e3), 1),
+        "launch_order_ms_per_step": round(ms_launch, 3),
+        "per_view_fp32": {"value": round(n_pix / (ms_pv / 1e3) / 1e6, 2), "unit": "Mpix/s",
+                          "ms_per_step": round(ms_pv, 3), "form": "FP32 plain drop-in, one call per view, tile 16",
+                          "stage_ms": stages_pv, "gpu_launches": int(launches_pv)},
+        "batch_over_per_view_fp32": round(ms_pv / ms_b, 3),
+        "stage_ms": stages_b, "gpu_launches": int(launches_b), "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -465,11 +620,18 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="tile size of the headline form (0 = autotune over 8, 16)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="mixture1m", choices=["mixture1m", "batch"],
+                    help="mixture1m: the headline workload; batch: 64 uneven views over 3 scenes (batching form)")
+    ap.add_argument("--views", type=int, default=64, help="views of the batch workload")
+    ap.add_argument("--tile-order", default="heaviest_first", choices=["launch", "heaviest_first"],
+                    help="compositor tile order of the headline form")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes of one compositor-adjoint launch from an ncu capture, reported as roofline.traffic")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -47,6 +47,22 @@ typedef struct CUstream_st* tg_stream_t; /* same type as cudaStream_t */
 #define TG_ADJ_BWD2 1      /* "bilinear_bwd2": reference UV term (du/ds factor (R-1)/range) */
 #define TG_ADJ_EXACT 2     /* exact derivative of the forward ((R-1)/(2*range)) */
 
+/* ------------------------------------------------------------------ batching form
+ * Views of uneven size in one call (no counterpart in the reference, which
+ * renders C cameras of one size per call).  A batch of C views is described by
+ * a device array tg_view[C]; the tiles of all views form one flat list (view c
+ * owns tiles [tile_base, tile_base + tile_width*tile_height), row-major), and
+ * the per-pixel outputs are flat over all views (view c owns pixels
+ * [pix_base, pix_base + width*height), row-major).  tile_view[t] is the view of
+ * flat tile t.  Kernels bounds-check every pixel and tile index against the
+ * totals passed beside the table. */
+typedef struct {
+    int32_t width, height;           /* image size of the view */
+    int32_t tile_width, tile_height; /* its tile grid: ceil(width / tile_size), ceil(height / tile_size) */
+    int64_t tile_base;               /* first flat tile of the view */
+    int64_t pix_base;                /* first flat pixel of the view */
+} tg_view;
+
 TG_API int tg_version(void);
 TG_API const char* tg_last_error(void);
 /* Number of kernels this library has launched in this process (all devices,
@@ -132,6 +148,13 @@ typedef struct {
     float* depths;          /* [nnz] (emit) */
     float* ray_transforms;  /* [nnz,3,3] (emit) */
     float* normals;         /* [nnz,3] (emit) */
+    /* Batching form (NULL / 0 otherwise): camera c projects only Gaussians
+     * [gauss_ranges[2c], gauss_ranges[2c+1]) (its scene inside the concatenated
+     * Gaussian arrays; max_range = the longest range) onto an image of
+     * views[c].width x views[c].height.  N is then the total Gaussian count. */
+    const tg_view* views;         /* [C] or NULL */
+    const int64_t* gauss_ranges;  /* [C,2] or NULL */
+    int32_t max_range;
 } tg_project_packed_args;
 TG_API size_t tg_project_packed_workspace_bytes(int32_t C, int32_t N);
 TG_API int tg_project_packed_count(const tg_project_packed_args* a, tg_stream_t stream);
@@ -186,6 +209,10 @@ typedef struct {
     void* scan_workspace;       /* tg_scan_workspace_bytes(n_elems) bytes */
     int64_t* isect_ids;         /* [n_isects] (emit only) */
     int32_t* flatten_ids;       /* [n_isects] (emit only) */
+    /* Batching form: per-camera tile grids (tile_width/tile_height above are
+     * then the largest grid's, which sets the tile bits of the keys); tile ids
+     * in the keys are local to the camera.  NULL: one grid for all cameras. */
+    const tg_view* views;       /* [n_cameras] or NULL */
 } tg_isect_args;
 TG_API size_t tg_scan_workspace_bytes(int64_t n_elems);
 TG_API int tg_isect_count(const tg_isect_args* a, tg_stream_t stream);
@@ -219,6 +246,14 @@ TG_API int tg_sort_pairs_noalloc(int64_t* keys, int32_t* vals, int64_t* keys_alt
  * or of the next non-empty tile. */
 TG_API int tg_isect_offset_encode(const int64_t* isect_ids, int64_t n_isects, int32_t n_cameras, int32_t tile_width,
                            int32_t tile_height, int32_t* offsets, tg_stream_t stream);
+
+/* Batching form of tg_isect_offset_encode: offsets[t] for every flat tile t of
+ * the views (n_tiles in total, tile_view[t] its view); max_tiles_per_view sets
+ * the tile bits of the keys, as in tg_isect_args.  No counterpart in the
+ * reference. */
+TG_API int tg_isect_offset_encode_views(const int64_t* isect_ids, int64_t n_isects, int32_t n_cameras,
+                                        int64_t max_tiles_per_view, const tg_view* views, const int32_t* tile_view,
+                                        int64_t n_tiles, int32_t* offsets, tg_stream_t stream);
 
 /* ------------------------------------------------------------------ compositor
  * Replaces rasterize_to_pixels_fwd_textured_gaussians_tensor
@@ -258,6 +293,16 @@ typedef struct {
     int32_t* median_ids;        /* [C,H,W] */
     float* contrib_sum;         /* [n_contrib] (zeroed by the call) */
     float* contrib_count;       /* [n_contrib] (zeroed by the call) */
+    /* Work order and batching form (all NULL / 0 for one image size in CTA order).
+     * tile_order: [n tiles] permutation giving the order in which tiles are
+     * taken (e.g. heaviest first), or NULL.  views / tile_view: the view table
+     * above; tile_offsets and masks are then [n_tiles] over the flat tile list,
+     * the per-pixel outputs [n_pixels, ...] over the flat pixels, backgrounds
+     * [C,D], and width/height/tile_width/tile_height are ignored. */
+    const int32_t* tile_order;
+    const tg_view* views;
+    const int32_t* tile_view;
+    int64_t n_tiles, n_pixels;
 } tg_raster_fwd_args;
 TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
 

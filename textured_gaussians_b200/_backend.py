@@ -43,7 +43,7 @@ class ProjectPackedArgs(ctypes.Structure):
                 ("width", I32), ("height", I32), ("near_plane", F32), ("far_plane", F32), ("radius_clip", F32),
                 ("workspace", P), ("nnz", P), ("indptr", P), ("nnz_host", I64), ("camera_ids", P),
                 ("gaussian_ids", P), ("radii", P), ("means2d", P), ("depths", P), ("ray_transforms", P),
-                ("normals", P)]
+                ("normals", P), ("views", P), ("gauss_ranges", P), ("max_range", I32)]
 
 
 class ProjectPackedBwdArgs(ctypes.Structure):
@@ -57,7 +57,7 @@ class IsectArgs(ctypes.Structure):
     _fields_ = [("n_elems", I64), ("N", I64), ("camera_ids", P), ("means2d", P), ("radii", P), ("depths", P),
                 ("tile_size", I32), ("tile_width", I32), ("tile_height", I32), ("n_cameras", I32),
                 ("tiles_per_gauss", P), ("cum_tiles", P), ("n_isects", P), ("scan_workspace", P),
-                ("isect_ids", P), ("flatten_ids", P)]
+                ("isect_ids", P), ("flatten_ids", P), ("views", P)]
 
 
 class RasterFwdArgs(ctypes.Structure):
@@ -68,7 +68,8 @@ class RasterFwdArgs(ctypes.Structure):
                 ("range_y", F32), ("backgrounds", P), ("masks", P), ("tile_offsets", P), ("flatten_ids", P),
                 ("gaussian_ids", P), ("contrib_threshold", F32), ("g_weight", F32), ("n_contrib", I32),
                 ("out_colors", P), ("out_alphas", P), ("out_normals", P), ("out_distort", P), ("out_median", P),
-                ("last_ids", P), ("median_ids", P), ("contrib_sum", P), ("contrib_count", P)]
+                ("last_ids", P), ("median_ids", P), ("contrib_sum", P), ("contrib_count", P), ("tile_order", P),
+                ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64)]
 
 
 class RasterBwdArgs(ctypes.Structure):
@@ -107,6 +108,7 @@ def lib() -> ctypes.CDLL:
                 ("tg_isect_emit", [ctypes.POINTER(IsectArgs), P]),
                 ("tg_sort_pairs", [P, P, P, P, I64, I32, P, ctypes.c_size_t, ctypes.POINTER(I32), P]),
                 ("tg_isect_offset_encode", [P, I64, I32, I32, I32, P, P]),
+                ("tg_isect_offset_encode_views", [P, I64, I32, I64, P, P, I64, P, P]),
                 ("tg_rasterize_fwd", [ctypes.POINTER(RasterFwdArgs), P]),
                 ("tg_rasterize_bwd", [ctypes.POINTER(RasterBwdArgs), P]),
                 ("tg_sh_fwd", [I64, I64, I32, I32, P, P, P, P, P]),

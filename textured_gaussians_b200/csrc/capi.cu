@@ -27,6 +27,9 @@ int sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_al
                void* workspace, size_t ws_bytes, int32_t* result_in_alt, cudaStream_t s, cudaError_t& cerr);
 cudaError_t launch_offset_encode(const int64_t* keys, int64_t n, int C, int tw, int th, int tile_n_bits, int end_bit,
                                  int32_t* offsets, cudaStream_t s);
+cudaError_t launch_offset_encode_views(const int64_t* keys, int64_t n, int C, int64_t n_tiles, const tg_view* views,
+                                       const int32_t* tile_view, int tile_n_bits, int end_bit, int32_t* offsets,
+                                       cudaStream_t s);
 cudaError_t launch_raster_fwd(const tg_raster_fwd_args& a, cudaStream_t s);
 cudaError_t launch_raster_bwd(const tg_raster_bwd_args& a, cudaStream_t s);
 cudaError_t launch_sh_fwd(int64_t n, int64_t rows, int degree, int K, const float* dirs, const float* coeffs,
@@ -79,13 +82,24 @@ namespace {
         if (!(cond)) return fail(code, __VA_ARGS__); \
     } while (0)
 
+int64_t raster_pixels(const tg_raster_fwd_args& a) {
+    return a.views ? a.n_pixels : (int64_t)a.C * a.height * a.width;
+}
+
 int check_raster_common(const tg_raster_fwd_args& a) {
     TG_REQUIRE(a.C >= 0 && a.width >= 0 && a.height >= 0, TG_ERR_INVALID_ARG, "negative sizes");
     TG_REQUIRE(a.tile_size == 16 || a.tile_size == 8, TG_ERR_UNSUPPORTED, "tile_size %d not supported (8 or 16)",
                a.tile_size);
     TG_REQUIRE(a.D >= 1 && a.D <= 5, TG_ERR_UNSUPPORTED, "unsupported number of channels: %d", a.D);
-    TG_REQUIRE((int64_t)a.tile_width * a.tile_size >= a.width && (int64_t)a.tile_height * a.tile_size >= a.height,
-               TG_ERR_INVALID_ARG, "tile grid %dx%d does not cover the image", a.tile_width, a.tile_height);
+    if (a.views) {
+        TG_REQUIRE(a.tile_view && a.n_tiles >= 0 && a.n_tiles < (int64_t(1) << 31) && a.n_pixels >= 0,
+                   TG_ERR_INVALID_ARG, "view table needs tile_view, n_tiles and n_pixels");
+    } else {
+        TG_REQUIRE((int64_t)a.tile_width * a.tile_size >= a.width && (int64_t)a.tile_height * a.tile_size >= a.height,
+                   TG_ERR_INVALID_ARG, "tile grid %dx%d does not cover the image", a.tile_width, a.tile_height);
+        TG_REQUIRE((int64_t)a.C * a.tile_width * a.tile_height < (int64_t(1) << 31), TG_ERR_INVALID_ARG,
+                   "too many tiles");
+    }
     TG_REQUIRE(a.n_isects >= 0 && a.n_isects < (int64_t(1) << 31), TG_ERR_INVALID_ARG, "n_isects out of range");
     TG_REQUIRE(a.tile_offsets && (a.n_isects == 0 || a.flatten_ids), TG_ERR_INVALID_ARG, "null offsets/flatten ids");
     TG_REQUIRE(a.means2d && a.ray_transforms && a.colors && a.opacities && a.normals, TG_ERR_INVALID_ARG,
@@ -155,6 +169,7 @@ int check_packed_common(const tg_project_packed_args* a) {
     TG_REQUIRE(a->C >= 0 && a->N >= 0, TG_ERR_INVALID_ARG, "negative sizes");
     TG_REQUIRE(a->C <= 65535, TG_ERR_UNSUPPORTED, "at most 65535 cameras (got %d)", a->C);
     TG_REQUIRE(a->workspace && a->nnz && a->indptr, TG_ERR_INVALID_ARG, "null workspace / nnz / indptr");
+    TG_REQUIRE(a->gauss_ranges == nullptr || a->max_range >= 0, TG_ERR_INVALID_ARG, "negative max_range");
     if ((int64_t)a->C * a->N == 0) return TG_OK;
     TG_REQUIRE(a->means && a->quats && a->scales && a->viewmats && a->Ks, TG_ERR_INVALID_ARG, "null pointer");
     TG_REQUIRE(aligned(a->quats, 16), TG_ERR_INVALID_ARG, "quats must be 16-byte aligned");
@@ -263,11 +278,27 @@ int tg_isect_offset_encode(const int64_t* isect_ids, int64_t n_isects, int32_t n
                        "tg_isect_offset_encode");
 }
 
+int tg_isect_offset_encode_views(const int64_t* isect_ids, int64_t n_isects, int32_t n_cameras,
+                                 int64_t max_tiles_per_view, const tg_view* views, const int32_t* tile_view,
+                                 int64_t n_tiles, int32_t* offsets, tg_stream_t stream) {
+    TG_REQUIRE(n_cameras > 0 && max_tiles_per_view > 0 && n_tiles >= 0 && n_tiles < (int64_t(1) << 31),
+               TG_ERR_INVALID_ARG, "bad sizes");
+    TG_REQUIRE(n_isects >= 0 && (n_isects == 0 || isect_ids), TG_ERR_INVALID_ARG, "null isect_ids");
+    if (n_tiles == 0) return TG_OK;
+    TG_REQUIRE(views && tile_view && offsets, TG_ERR_INVALID_ARG, "null view table or offsets");
+    const int tb = bit_width(max_tiles_per_view);
+    const int cb = bit_width(n_cameras);
+    TG_REQUIRE(tb + cb <= 32, TG_ERR_INVALID_ARG, "camera and tile ids need more than 32 bits");
+    return cuda_status(tg::launch_offset_encode_views(isect_ids, n_isects, n_cameras, n_tiles, views, tile_view, tb,
+                                                      32 + tb + cb, offsets, stream),
+                       "tg_isect_offset_encode_views");
+}
+
 int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream) {
     TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
     int rc = check_raster_common(*a);
     if (rc != TG_OK) return rc;
-    const int64_t pixels = (int64_t)a->C * a->height * a->width;
+    const int64_t pixels = raster_pixels(*a);
     if (pixels > 0)
         TG_REQUIRE(a->out_colors && a->out_alphas && a->out_normals && a->out_distort && a->out_median &&
                        a->last_ids && a->median_ids,

@@ -31,6 +31,20 @@ __device__ __forceinline__ void tile_box(float mx, float my, int32_t radius, int
     y1 = min((uint32_t)ceilf(ty + tr), th);
 }
 
+// Camera of element e and its tile grid; false if the camera id is out of range.
+__device__ __forceinline__ bool camera_grid(const tg_isect_args& a, int64_t e, uint32_t& tw, uint32_t& th) {
+    const int64_t cid = a.camera_ids ? a.camera_ids[e] : e / a.N;
+    if (cid < 0 || cid >= a.n_cameras) return false;
+    if (a.views) {
+        tw = (uint32_t)a.views[cid].tile_width;
+        th = (uint32_t)a.views[cid].tile_height;
+    } else {
+        tw = (uint32_t)a.tile_width;
+        th = (uint32_t)a.tile_height;
+    }
+    return true;
+}
+
 // Phase 1: tile counts per element and per-chunk sums.
 __global__ void __launch_bounds__(kScanThreads) isect_count_kernel(tg_isect_args a, int64_t* chunk_sums) {
     __shared__ int64_t s_warp[kScanThreads / 32];
@@ -42,10 +56,11 @@ __global__ void __launch_bounds__(kScanThreads) isect_count_kernel(tg_isect_args
         if (e >= a.n_elems) break;
         int32_t cnt = 0;
         const int32_t r = a.radii[e];
-        if (r > 0) {
+        uint32_t tw, th;
+        if (r > 0 && camera_grid(a, e, tw, th)) {
             const float2 m = reinterpret_cast<const float2*>(a.means2d)[e];
             uint32_t x0, y0, x1, y1;
-            tile_box(m.x, m.y, r, a.tile_size, a.tile_width, a.tile_height, x0, y0, x1, y1);
+            tile_box(m.x, m.y, r, a.tile_size, tw, th, x0, y0, x1, y1);
             cnt = (int32_t)((y1 - y0) * (x1 - x0));
         }
         a.tiles_per_gauss[e] = cnt;
@@ -106,17 +121,18 @@ __global__ void __launch_bounds__(256) isect_emit_kernel(tg_isect_args a, int ti
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.n_elems) return;
     const int32_t r = a.radii[e];
-    if (r <= 0) return;
+    uint32_t tw, th;
+    if (r <= 0 || !camera_grid(a, e, tw, th)) return;
     const float2 m = reinterpret_cast<const float2*>(a.means2d)[e];
     uint32_t x0, y0, x1, y1;
-    tile_box(m.x, m.y, r, a.tile_size, a.tile_width, a.tile_height, x0, y0, x1, y1);
+    tile_box(m.x, m.y, r, a.tile_size, tw, th, x0, y0, x1, y1);
     const int64_t cid = a.camera_ids ? a.camera_ids[e] : e / a.N;
     const int64_t cid_enc = cid << (32 + tile_n_bits);
     const int64_t depth_enc = (int64_t)__float_as_int(a.depths[e]);  // sign-extended like the reference
     int64_t cur = e == 0 ? 0 : a.cum_tiles[e - 1];
     for (uint32_t y = y0; y < y1; ++y)
         for (uint32_t x = x0; x < x1; ++x) {
-            const int64_t tile_id = (int64_t)y * a.tile_width + x;
+            const int64_t tile_id = (int64_t)y * tw + x;
             a.isect_ids[cur] = cid_enc | (tile_id << 32) | depth_enc;
             a.flatten_ids[cur] = (int32_t)e;
             ++cur;
@@ -136,6 +152,26 @@ __global__ void __launch_bounds__(256) offset_encode_kernel(const int64_t* keys,
         const uint64_t h = ((uint64_t)__ldg(keys + mid) & key_mask) >> 32;
         const int64_t id = (int64_t)(h >> tile_n_bits) * n_tiles + (int64_t)(h & tmask);
         if (id < t) lo = mid + 1; else hi = mid;
+    }
+    offsets[t] = (int32_t)lo;
+}
+
+// Batching form: flat tile t of view c = tile_view[t] is the key prefix
+// (c << tile_bits) | (t - tile_base_c); offsets[t] = its lower bound.
+__global__ void __launch_bounds__(256) offset_encode_views_kernel(const int64_t* keys, int64_t n, int64_t n_tiles,
+                                                                  int C, const tg_view* views,
+                                                                  const int32_t* tile_view, int tile_n_bits,
+                                                                  uint64_t key_mask, int32_t* offsets) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tiles) return;
+    const int c = tile_view[t];
+    uint64_t target = ~0ull;  // an out-of-range view sorts after every key
+    if (c >= 0 && c < C) target = ((uint64_t)c << tile_n_bits) | (uint64_t)(t - views[c].tile_base);
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        const uint64_t h = ((uint64_t)__ldg(keys + mid) & key_mask) >> 32;
+        if (h < target) lo = mid + 1; else hi = mid;
     }
     offsets[t] = (int32_t)lo;
 }
@@ -413,6 +449,17 @@ cudaError_t launch_isect_count(const tg_isect_args& a, cudaStream_t s) {
 cudaError_t launch_isect_emit(const tg_isect_args& a, int tile_n_bits, cudaStream_t s) {
     if (a.n_elems == 0) return cudaSuccess;
     isect_emit_kernel<<<(unsigned)((a.n_elems + 255) / 256), 256, 0, s>>>(a, tile_n_bits);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_offset_encode_views(const int64_t* keys, int64_t n, int C, int64_t n_tiles, const tg_view* views,
+                                       const int32_t* tile_view, int tile_n_bits, int end_bit, int32_t* offsets,
+                                       cudaStream_t s) {
+    if (n_tiles == 0) return cudaSuccess;
+    const uint64_t key_mask = end_bit >= 64 ? ~0ull : ((1ull << end_bit) - 1ull);
+    offset_encode_views_kernel<<<(unsigned)((n_tiles + 255) / 256), 256, 0, s>>>(keys, n, n_tiles, C, views, tile_view,
+                                                                                tile_n_bits, key_mask, offsets);
     note_launches(1);
     return cudaGetLastError();
 }

@@ -118,22 +118,42 @@ constexpr int kPackThreads = 256;
 constexpr int kPackItems = 16;
 constexpr int kPackChunk = kPackThreads * kPackItems;  // entries of one camera row per CTA
 
-__device__ __forceinline__ int64_t pack_rows(int32_t N) { return ((int64_t)N + kPackChunk - 1) / kPackChunk; }
+// Row of camera c: Gaussians [g0, g0 + len) (all N, or the camera's scene in
+// the batching form, clamped to [0, N)) and its image size.
+struct PackRow {
+    int64_t g0, len;
+    int32_t width, height;
+};
+__device__ __forceinline__ PackRow pack_row(const tg_project_packed_args& a, int c) {
+    PackRow r{0, a.N, a.width, a.height};
+    if (a.gauss_ranges) {
+        const int64_t b = min(max(a.gauss_ranges[2 * c], (int64_t)0), (int64_t)a.N);
+        const int64_t e = min(max(a.gauss_ranges[2 * c + 1], b), (int64_t)a.N);
+        r.g0 = b;
+        r.len = e - b;
+    }
+    if (a.views) {
+        r.width = a.views[c].width;
+        r.height = a.views[c].height;
+    }
+    return r;
+}
 
 // Pass 1: number of visible entries in each chunk (blockIdx.x) of camera blockIdx.y.
 __global__ void __launch_bounds__(kPackThreads) project_packed_count_kernel(tg_project_packed_args a,
                                                                            int64_t* chunk_counts) {
     __shared__ int64_t s_warp[kPackThreads / 32];
     const int c = blockIdx.y;
+    const PackRow row = pack_row(a, c);
     const int64_t base = (int64_t)blockIdx.x * kPackChunk;
     int64_t local = 0;
 #pragma unroll 1
     for (int i = 0; i < kPackItems; ++i) {
-        const int64_t n = base + (int64_t)i * kPackThreads + threadIdx.x;
-        if (n >= a.N) break;
+        const int64_t k = base + (int64_t)i * kPackThreads + threadIdx.x;
+        if (k >= row.len) break;
         Projected o;
-        local += project_one(a.means, a.quats, a.scales, a.viewmats, a.Ks, a.width, a.height, a.near_plane,
-                             a.far_plane, a.radius_clip, c, n, o);
+        local += project_one(a.means, a.quats, a.scales, a.viewmats, a.Ks, row.width, row.height, a.near_plane,
+                             a.far_plane, a.radius_clip, c, row.g0 + k, o);
     }
     int64_t total;
     block_excl_scan(local, s_warp, total);
@@ -156,17 +176,19 @@ __global__ void __launch_bounds__(kPackThreads) project_packed_emit_kernel(tg_pr
                                                                           const int64_t* chunk_offsets) {
     __shared__ int32_t s_warp[kPackThreads / 32];
     const int c = blockIdx.y;
+    const PackRow row = pack_row(a, c);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t base = (int64_t)blockIdx.x * kPackChunk;
     int64_t run = chunk_offsets[(int64_t)c * gridDim.x + blockIdx.x];
 #pragma unroll 1
     for (int i = 0; i < kPackItems; ++i) {
         const int64_t slice = base + (int64_t)i * kPackThreads;
-        if (slice >= a.N) break;  // uniform across the CTA
-        const int64_t n = slice + threadIdx.x;
+        if (slice >= row.len) break;  // uniform across the CTA
+        const int64_t k = slice + threadIdx.x;
+        const int64_t n = row.g0 + k;
         Projected o;
-        const bool vis = n < a.N && project_one(a.means, a.quats, a.scales, a.viewmats, a.Ks, a.width, a.height,
-                                                a.near_plane, a.far_plane, a.radius_clip, c, n, o);
+        const bool vis = k < row.len && project_one(a.means, a.quats, a.scales, a.viewmats, a.Ks, row.width,
+                                                    row.height, a.near_plane, a.far_plane, a.radius_clip, c, n, o);
         const unsigned ballot = __ballot_sync(0xffffffffu, vis);
         if (lane == 0) s_warp[warp] = __popc(ballot);
         __syncthreads();
@@ -375,10 +397,16 @@ size_t project_packed_workspace_bytes(int32_t C, int32_t N) {
     return align256(sizeof(int64_t) * (size_t)std::max<int64_t>(chunks, 1));
 }
 
+// Chunks per camera row: the longest row over 4096.
+inline int64_t packed_chunks_per_row(const tg_project_packed_args& a) {
+    const int64_t len = a.gauss_ranges ? std::min<int64_t>(a.max_range, a.N) : a.N;
+    return (len + kPackChunk - 1) / kPackChunk;
+}
+
 // Count pass: chunk counts, their scan (-> *nnz), indptr.  Three launches.
 cudaError_t launch_project_packed_count(const tg_project_packed_args& a, cudaStream_t s) {
-    const int64_t per_row = ((int64_t)a.N + kPackChunk - 1) / kPackChunk;
-    if ((int64_t)a.C * a.N == 0) {
+    const int64_t per_row = packed_chunks_per_row(a);
+    if ((int64_t)a.C * per_row == 0) {
         cudaError_t e = cudaMemsetAsync(a.nnz, 0, sizeof(int64_t), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(a.indptr, 0, sizeof(int32_t) * ((size_t)a.C + 1), s);
         return e;
@@ -397,8 +425,8 @@ cudaError_t launch_project_packed_count(const tg_project_packed_args& a, cudaStr
 
 // Emit pass; the chunk offsets left in the workspace by the count pass are reused.
 cudaError_t launch_project_packed_emit(const tg_project_packed_args& a, cudaStream_t s) {
-    const int64_t per_row = ((int64_t)a.N + kPackChunk - 1) / kPackChunk;
-    if ((int64_t)a.C * a.N == 0 || a.nnz_host == 0) return cudaSuccess;
+    const int64_t per_row = packed_chunks_per_row(a);
+    if ((int64_t)a.C * per_row == 0 || a.nnz_host == 0) return cudaSuccess;
     project_packed_emit_kernel<<<dim3((unsigned)per_row, (unsigned)a.C), kPackThreads, 0, s>>>(
         a, static_cast<const int64_t*>(a.workspace));
     note_launches(1);

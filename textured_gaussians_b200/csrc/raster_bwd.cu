@@ -217,15 +217,14 @@ __global__ void __launch_bounds__(256 / PPT, TG_BWD_MIN_CTAS) raster_bwd_kernel(
     __shared__ int s_max_bin;
 
     const unsigned wmask = __activemask();
-    const TileCoord tc = tile_of_block(f.tile_width, f.tile_height);
+    const TileWork tc = tile_work(f, blockIdx.x);
+    if (!tc.valid) return;  // uniform over the CTA
     const int tr = threadIdx.x, lane = tr & 31;
-    const int per_cam = f.tile_width * f.tile_height;
-    if (f.masks != nullptr && !f.masks[(int64_t)tc.c * per_cam + tc.tile]) return;
+    if (f.masks != nullptr && !f.masks[tc.t]) return;
 
     const int ts = f.tile_size;
-    const int64_t toff = (int64_t)tc.c * per_cam + tc.tile;
-    const int32_t range_start = f.tile_offsets[toff];
-    const int32_t range_end = (tc.c == f.C - 1 && tc.tile == per_cam - 1) ? (int32_t)f.n_isects : f.tile_offsets[toff + 1];
+    const int32_t range_start = tc.range_start;
+    const int32_t range_end = tc.range_end;
 
     // pixel-centre rectangle covered by this warp (for the warp-level cull)
     float wx0 = INFINITY, wx1 = -INFINITY, wy0 = INFINITY, wy1 = -INFINITY;
@@ -251,8 +250,8 @@ __global__ void __launch_bounds__(256 / PPT, TG_BWD_MIN_CTAS) raster_bwd_kernel(
         const int local = tr + q * nt;
         const int i = tc.ty * ts + local / ts;
         const int j = tc.tx * ts + local % ts;
-        p.inside = i < f.height && j < f.width;
-        p.pix = ((int64_t)tc.c * f.height + i) * f.width + j;
+        p.pix = pixel_index(tc, i, j);
+        p.inside = p.pix >= 0;
         p.px = (float)j + 0.5f;
         p.py = (float)i + 0.5f;
         p.T_final = 1.f; p.v_a = p.v_dist = p.v_med = p.bg_dot = 0.f;
@@ -389,7 +388,7 @@ cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     const int tile_px = f.tile_size * f.tile_size;
     const size_t smem = (size_t)tile_px * (6 * sizeof(float4) + D * sizeof(float) + 2 * sizeof(int) +
                                            GradSlots<D>::kCount * sizeof(float));
-    const int64_t blocks = (int64_t)f.C * f.tile_width * f.tile_height;
+    const int64_t blocks = f.views ? f.n_tiles : (int64_t)f.C * f.tile_width * f.tile_height;
     const float uv_scale = a.adjoint == TG_ADJ_BWD2 ? 1.f : (a.adjoint == TG_ADJ_EXACT ? 0.5f : 0.f);
     const bool multi = tile_px >= 64 * TG_BWD_PPT;
     cudaError_t err = multi ? cudaFuncSetAttribute(raster_bwd_kernel<D, Tex, TG_BWD_PPT>,

@@ -169,17 +169,63 @@ __device__ __forceinline__ float warp_sum(float v, unsigned mask) {
     return v;
 }
 
-struct TileCoord {
-    int c, ty, tx, tile;
+// The tile a CTA works on and the image it belongs to.  Work item `item`
+// (blockIdx.x) maps to flat tile tile_order[item] (or item); the flat tile
+// maps to (view, tile x, tile y) through the view table in the batching form,
+// or through the one tile grid otherwise.  valid is false for an item whose
+// tile or view index is out of range (the CTA then does nothing).
+struct TileWork {
+    int c, tx, ty;
+    int64_t t;
+    int width, height;
+    int64_t pix_base;   // first flat pixel of the view
+    int64_t pix_limit;  // pixels of all views: every pixel index is checked against it
+    int32_t range_start, range_end;
+    bool valid;
 };
-__device__ __forceinline__ TileCoord tile_of_block(int tile_w, int tile_h) {
-    TileCoord t;
-    const int per_cam = tile_w * tile_h;
-    t.c = blockIdx.x / per_cam;
-    t.tile = blockIdx.x - t.c * per_cam;
-    t.ty = t.tile / tile_w;
-    t.tx = t.tile - t.ty * tile_w;
-    return t;
+
+__device__ __forceinline__ TileWork tile_work(const tg_raster_fwd_args& a, int64_t item) {
+    TileWork w;
+    const int64_t per_cam = (int64_t)a.tile_width * a.tile_height;
+    const int64_t n_tiles = a.views ? a.n_tiles : (int64_t)a.C * per_cam;
+    w.t = a.tile_order ? (int64_t)a.tile_order[item] : item;
+    w.valid = w.t >= 0 && w.t < n_tiles;
+    if (!w.valid) return w;
+    if (a.views) {
+        w.c = a.tile_view[w.t];
+        w.valid = w.c >= 0 && w.c < a.C;
+        if (!w.valid) return w;
+        const tg_view v = a.views[w.c];
+        const int64_t local = w.t - v.tile_base;
+        w.valid = v.tile_width > 0 && local >= 0 && local < (int64_t)v.tile_width * v.tile_height;
+        if (!w.valid) return w;
+        w.ty = (int)(local / v.tile_width);
+        w.tx = (int)(local - (int64_t)w.ty * v.tile_width);
+        w.width = v.width;
+        w.height = v.height;
+        w.pix_base = v.pix_base;
+        w.pix_limit = a.n_pixels;
+    } else {
+        w.c = (int)(w.t / per_cam);
+        const int64_t local = w.t - (int64_t)w.c * per_cam;
+        w.ty = (int)(local / a.tile_width);
+        w.tx = (int)(local - (int64_t)w.ty * a.tile_width);
+        w.width = a.width;
+        w.height = a.height;
+        w.pix_base = (int64_t)w.c * a.height * a.width;
+        w.pix_limit = (int64_t)a.C * a.height * a.width;
+    }
+    w.range_start = a.tile_offsets[w.t];
+    w.range_end = w.t == n_tiles - 1 ? (int32_t)a.n_isects : a.tile_offsets[w.t + 1];
+    return w;
+}
+
+// Flat index of pixel (i, j) of the work item's view, or -1 outside the view
+// or the flat outputs.
+__device__ __forceinline__ int64_t pixel_index(const TileWork& w, int i, int j) {
+    if (i >= w.height || j >= w.width) return -1;
+    const int64_t p = w.pix_base + (int64_t)i * w.width + j;
+    return (p >= 0 && p < w.pix_limit) ? p : -1;
 }
 
 }  // namespace tg

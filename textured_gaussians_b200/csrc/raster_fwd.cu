@@ -1,6 +1,6 @@
 // Textured / plain 2DGS compositor, forward, for sm_100a.
 //
-// One CTA per (camera, tile), front-to-back over the tile's depth-sorted
+// One CTA per (camera, tile) work item, front-to-back over the tile's depth-sorted
 // splats in batches of tile_size^2 splats staged in shared memory (the gather
 // of each splat's record happens once per CTA, not once per pixel).  Each
 // thread owns PPT pixels of the tile (rows r and r + tile/PPT): the PPT
@@ -46,10 +46,10 @@ __global__ void __launch_bounds__(256 / PPT, TG_FWD_MIN_CTAS) raster_fwd_kernel(
     int* s_row = reinterpret_cast<int*>(s_col + bs * D);
 
     const unsigned wmask = __activemask();
-    const TileCoord tc = tile_of_block(a.tile_width, a.tile_height);
+    const TileWork tc = tile_work(a, blockIdx.x);
+    if (!tc.valid) return;  // uniform over the CTA
     const int tr = threadIdx.x, lane = tr & 31;
     const int ts = a.tile_size;
-    const int per_cam = a.tile_width * a.tile_height;
 
     int64_t pix[PPT];
     bool inside[PPT], done[PPT];
@@ -59,14 +59,14 @@ __global__ void __launch_bounds__(256 / PPT, TG_FWD_MIN_CTAS) raster_fwd_kernel(
         const int local = tr + q * nt;
         const int i = tc.ty * ts + local / ts;
         const int j = tc.tx * ts + local % ts;
-        inside[q] = i < a.height && j < a.width;
-        pix[q] = ((int64_t)tc.c * a.height + i) * a.width + j;
+        pix[q] = pixel_index(tc, i, j);
+        inside[q] = pix[q] >= 0;
         px[q] = (float)j + 0.5f;
         py[q] = (float)i + 0.5f;
         done[q] = !inside[q];
     }
 
-    if (a.masks != nullptr && !a.masks[(int64_t)tc.c * per_cam + tc.tile]) {
+    if (a.masks != nullptr && !a.masks[tc.t]) {
 #pragma unroll
         for (int q = 0; q < PPT; ++q) {
             if (!inside[q]) continue;
@@ -96,9 +96,8 @@ __global__ void __launch_bounds__(256 / PPT, TG_FWD_MIN_CTAS) raster_fwd_kernel(
         wx0 = fminf(wx0, __shfl_xor_sync(wmask, wx0, o)); wx1 = fmaxf(wx1, __shfl_xor_sync(wmask, wx1, o));
         wy0 = fminf(wy0, __shfl_xor_sync(wmask, wy0, o)); wy1 = fmaxf(wy1, __shfl_xor_sync(wmask, wy1, o));
     }
-    const int64_t toff = (int64_t)tc.c * per_cam + tc.tile;
-    const int32_t range_start = a.tile_offsets[toff];
-    const int32_t range_end = (tc.c == a.C - 1 && tc.tile == per_cam - 1) ? (int32_t)a.n_isects : a.tile_offsets[toff + 1];
+    const int32_t range_start = tc.range_start;
+    const int32_t range_end = tc.range_end;
     const int num_batches = (range_end - range_start + bs - 1) / bs;
     const int64_t tex_stride = (int64_t)a.tex_ry * a.tex_rx;
 
@@ -224,7 +223,7 @@ template <int D, class Tex>
 cudaError_t launch_fwd_t(const tg_raster_fwd_args& a, cudaStream_t s) {
     const int tile_px = a.tile_size * a.tile_size;
     const size_t smem = (size_t)tile_px * (6 * sizeof(float4) + D * sizeof(float) + sizeof(int));
-    const int64_t blocks = (int64_t)a.C * a.tile_width * a.tile_height;
+    const int64_t blocks = a.views ? a.n_tiles : (int64_t)a.C * a.tile_width * a.tile_height;
     if (blocks == 0) return cudaSuccess;
     if (tile_px >= 64 * TG_FWD_PPT) {
         raster_fwd_kernel<D, Tex, TG_FWD_PPT><<<(unsigned)blocks, tile_px / TG_FWD_PPT, smem, s>>>(a);

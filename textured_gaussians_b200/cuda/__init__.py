@@ -2,6 +2,7 @@
 from ._wrapper import (
     fully_fused_projection_2dgs,
     isect_offset_encode,
+    isect_offset_encode_views,
     isect_tiles,
     make_texture_storage,
     rasterize_to_pixels_2dgs,
@@ -9,11 +10,13 @@ from ._wrapper import (
     sort_pairs,
     spherical_harmonics,
     spherical_harmonics_shared,
+    tile_order_heaviest_first,
 )
 
 __all__ = [
     "fully_fused_projection_2dgs",
     "isect_offset_encode",
+    "isect_offset_encode_views",
     "isect_tiles",
     "make_texture_storage",
     "rasterize_to_pixels_2dgs",
@@ -21,4 +24,5 @@ __all__ = [
     "sort_pairs",
     "spherical_harmonics",
     "spherical_harmonics_shared",
+    "tile_order_heaviest_first",
 ]

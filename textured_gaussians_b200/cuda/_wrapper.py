@@ -166,7 +166,7 @@ def fully_fused_projection_2dgs(
     if packed:
         return _FullyFusedProjectionPacked2DGS.apply(
             means.contiguous(), quats.contiguous(), scales.contiguous(), viewmats.contiguous(), Ks.contiguous(),
-            width, height, eps2d, near_plane, far_plane, radius_clip, sparse_grad, mode)
+            width, height, eps2d, near_plane, far_plane, radius_clip, sparse_grad, mode, None)
     return _FullyFusedProjection2DGS.apply(
         means.contiguous(), quats.contiguous(), scales.contiguous(), viewmats.contiguous(), Ks.contiguous(),
         width, height, eps2d, near_plane, far_plane, radius_clip, mode)
@@ -234,7 +234,7 @@ class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, means, quats, scales, viewmats, Ks, width, height, eps2d, near_plane, far_plane, radius_clip,
-                sparse_grad, mode):
+                sparse_grad, mode, batch):
         C, N = viewmats.shape[0], means.shape[0]
         dev = means.device
         ws = torch.empty((B.lib().tg_project_packed_workspace_bytes(C, N),), dtype=torch.uint8, device=dev)
@@ -243,6 +243,8 @@ class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
         a = B.ProjectPackedArgs(C, N, B.ptr(means), B.ptr(quats), B.ptr(scales), B.ptr(viewmats), B.ptr(Ks),
                                 int(width), int(height), float(near_plane), float(far_plane), float(radius_clip),
                                 B.ptr(ws), B.ptr(nnz_dev), B.ptr(indptr), 0)
+        if batch is not None:  # (view table bytes, [C,2] Gaussian ranges, longest range)
+            a.views, a.gauss_ranges, a.max_range = B.ptr(batch[0]), B.ptr(batch[1]), int(batch[2])
         st = B.stream_of(means)
         B.call("tg_project_packed_count", st, B.lib().tg_project_packed_count, ctypes.byref(a), st)
         nnz = int(nnz_dev.item())  # the one host synchronisation, as in the reference
@@ -300,7 +302,7 @@ class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
         v_viewmats = torch.zeros_like(viewmats) if ctx.needs_input_grad[4] else None
         return (out(v_means, means, ctx.needs_input_grad[0]), out(v_quats, quats, ctx.needs_input_grad[1]),
                 out(v_scales, scales, ctx.needs_input_grad[2]), v_viewmats,
-                None, None, None, None, None, None, None, None, None)
+                None, None, None, None, None, None, None, None, None, None)
 
 
 # --------------------------------------------------------------------------- intersection
@@ -317,12 +319,19 @@ def isect_tiles(
     n_cameras: Optional[int] = None,
     camera_ids: Optional[Tensor] = None,
     gaussian_ids: Optional[Tensor] = None,
+    *,
+    view_table=None,
 ) -> Tuple[Tensor, Tensor, Tensor]:
     """Maps projected Gaussians to intersecting tiles (reference: cuda/_wrapper.py:349-420).
 
     Returns ``(tiles_per_gauss int32 [C,N] or [nnz], isect_ids int64 [n_isects],
     flatten_ids int32 [n_isects])``, sorted stably by isect id when ``sort``.
+    ``view_table`` (batching form, :class:`textured_gaussians_b200.batch.ViewTable`)
+    gives every camera its own tile grid; tile_width / tile_height are then
+    ignored and the key's tile bits come from the largest grid.
     """
+    if view_table is not None:
+        tile_width, tile_height = view_table.key_tiles, 1
     if packed:
         nnz = means2d.size(0)
         assert means2d.shape == (nnz, 2), means2d.size()
@@ -349,7 +358,8 @@ def isect_tiles(
     n_dev = torch.empty((1,), dtype=torch.int64, device=dev)
     ws = torch.empty((B.lib().tg_scan_workspace_bytes(E),), dtype=torch.uint8, device=dev)
     a = B.IsectArgs(E, N, B.ptr(cam), B.ptr(means2d), B.ptr(radii), B.ptr(depths), int(tile_size), int(tile_width),
-                    int(tile_height), int(C), B.ptr(tiles_per_gauss), B.ptr(cum), B.ptr(n_dev), B.ptr(ws), None, None)
+                    int(tile_height), int(C), B.ptr(tiles_per_gauss), B.ptr(cum), B.ptr(n_dev), B.ptr(ws), None, None,
+                    None if view_table is None else B.ptr(view_table.views))
     stream = B.stream_of(means2d)
     B.call("tg_isect_count", stream, B.lib().tg_isect_count, ctypes.byref(a), stream)
     n_isects = int(n_dev.item())  # the one host synchronisation, as in the reference
@@ -390,6 +400,33 @@ def isect_offset_encode(isect_ids: Tensor, n_cameras: int, tile_width: int, tile
     B.call("tg_isect_offset_encode", st, B.lib().tg_isect_offset_encode, B.ptr(isect_ids), isect_ids.numel(),
            int(n_cameras), int(tile_width), int(tile_height), B.ptr(offsets), st)
     return offsets
+
+
+@torch.no_grad()
+def isect_offset_encode_views(isect_ids: Tensor, view_table) -> Tensor:
+    """Batching form of :func:`isect_offset_encode`: one offset per flat tile of
+    all views ([n_tiles] int32)."""
+    vt = view_table
+    isect_ids = isect_ids.contiguous()
+    offsets = torch.empty((vt.n_tiles,), dtype=torch.int32, device=isect_ids.device)
+    st = B.stream_of(isect_ids)
+    B.call("tg_isect_offset_encode_views", st, B.lib().tg_isect_offset_encode_views, B.ptr(isect_ids),
+           isect_ids.numel(), vt.n_views, vt.key_tiles, B.ptr(vt.views), B.ptr(vt.tile_view), vt.n_tiles,
+           B.ptr(offsets), st)
+    return offsets
+
+
+@torch.no_grad()
+def tile_order_heaviest_first(isect_offsets: Tensor, n_isects: int) -> Tensor:
+    """Permutation of the flat tiles by descending intersection count (stable),
+    so the longest tiles start first and the tail of the launch is short."""
+    flat = isect_offsets.reshape(-1).to(torch.int64)
+    n = flat.numel()
+    counts = torch.diff(flat, append=torch.tensor([n_isects], dtype=torch.int64, device=flat.device))
+    keys = ((1 << 31) - 1) - counts.clamp(0, (1 << 31) - 1)
+    vals = torch.arange(n, dtype=torch.int32, device=flat.device)
+    _, order = sort_pairs(keys.contiguous(), vals, 31)
+    return order
 
 
 # --------------------------------------------------------------------------- compositor
@@ -446,9 +483,12 @@ def make_texture_storage(textures: Tensor, fmt: str) -> Tuple[Tensor, Optional[T
 
 def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_store, tex_scales, range_x, range_y,
               backgrounds, masks, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-              gs_contrib_threshold, g_weight, C, N):
+              gs_contrib_threshold, g_weight, C, N, layout=None):
     D = colors.shape[-1]
-    th, tw = isect_offsets.shape[1:3]
+    vt = None if layout is None else layout.get("view_table")
+    th, tw = (1, 1) if vt is not None else isect_offsets.shape[1:3]
+    if vt is not None:
+        width = height = 0
     if textures_store is None:
         fmt, ry, rx = B.TG_TEX_NONE, 0, 0
     else:
@@ -458,7 +498,10 @@ def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_stor
         B.ptr(ray_transforms), B.ptr(colors), B.ptr(opacities), B.ptr(normals), fmt, B.ptr(textures_store),
         B.ptr(tex_scales), ry, rx, float(range_x), float(range_y), B.ptr(backgrounds), B.ptr(masks),
         B.ptr(isect_offsets), B.ptr(flatten_ids), B.ptr(gaussian_ids), float(gs_contrib_threshold), float(g_weight),
-        int(n_contrib), None, None, None, None, None, None, None, None, None)
+        int(n_contrib), None, None, None, None, None, None, None, None, None,
+        None if layout is None else B.ptr(layout.get("tile_order")),
+        None if vt is None else B.ptr(vt.views), None if vt is None else B.ptr(vt.tile_view),
+        0 if vt is None else vt.n_tiles, 0 if vt is None else vt.n_pixels)
 
 
 class _RasterizeToPixelsTextured(torch.autograd.Function):
@@ -472,9 +515,12 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
     @staticmethod
     def forward(ctx, means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, masks,
                 tex_store, tex_scales, range_x, range_y, width, height, tile_size, isect_offsets, flatten_ids,
-                absgrad, gs_contrib_threshold, g_weight, adjoint, bg_grad_index_ok, gaussian_ids, n_rows):
+                absgrad, gs_contrib_threshold, g_weight, adjoint, bg_grad_index_ok, gaussian_ids, n_rows, layout):
         dev = means2d.device
-        C = isect_offsets.shape[0]
+        vt = None if layout is None else layout.get("view_table")
+        C = isect_offsets.shape[0] if vt is None else vt.n_views
+        # per-pixel output shape: [C, H, W] for one image size, [n_pixels] over the flat views
+        pshape = (C, height, width) if vt is None else (vt.n_pixels,)
         # N: row modulus of the dense layout, or the packed entry count (row = entry) without gaussian_ids
         N = means2d.shape[1] if means2d.dim() == 3 else means2d.shape[0]
         n_contrib = N if gaussian_ids is None else n_rows
@@ -482,14 +528,14 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         m = None if masks is None else masks.to(torch.uint8).contiguous()
         a = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
                       backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-                      gs_contrib_threshold, g_weight, C, N)
-        render_colors = torch.empty((C, height, width, D), dtype=torch.float32, device=dev)
-        render_alphas = torch.empty((C, height, width, 1), dtype=torch.float32, device=dev)
-        render_normals = torch.empty((C, height, width, 3), dtype=torch.float32, device=dev)
-        render_distort = torch.empty((C, height, width, 1), dtype=torch.float32, device=dev)
-        render_median = torch.empty((C, height, width, 1), dtype=torch.float32, device=dev)
-        last_ids = torch.empty((C, height, width), dtype=torch.int32, device=dev)
-        median_ids = torch.empty((C, height, width), dtype=torch.int32, device=dev)
+                      gs_contrib_threshold, g_weight, C, N, layout)
+        render_colors = torch.empty(pshape + (D,), dtype=torch.float32, device=dev)
+        render_alphas = torch.empty(pshape + (1,), dtype=torch.float32, device=dev)
+        render_normals = torch.empty(pshape + (3,), dtype=torch.float32, device=dev)
+        render_distort = torch.empty(pshape + (1,), dtype=torch.float32, device=dev)
+        render_median = torch.empty(pshape + (1,), dtype=torch.float32, device=dev)
+        last_ids = torch.empty(pshape, dtype=torch.int32, device=dev)
+        median_ids = torch.empty(pshape, dtype=torch.int32, device=dev)
         contrib_sum = torch.empty((n_contrib,), dtype=torch.float32, device=dev)
         contrib_count = torch.empty((n_contrib,), dtype=torch.float32, device=dev)
         a.out_colors, a.out_alphas, a.out_normals = B.ptr(render_colors), B.ptr(render_alphas), B.ptr(render_normals)
@@ -502,7 +548,8 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
                               tex_store, tex_scales, isect_offsets, flatten_ids, render_colors, render_alphas,
                               last_ids, median_ids, gaussian_ids)
         ctx.cfg = (range_x, range_y, width, height, tile_size, absgrad, g_weight, adjoint, bg_grad_index_ok,
-                   gs_contrib_threshold, N, n_contrib)
+                   gs_contrib_threshold, N, n_contrib, C, pshape)
+        ctx.layout = layout
         ctx.mark_non_differentiable(contrib_sum, contrib_count)
         return render_colors, render_alphas, render_normals, render_distort, render_median, contrib_sum, contrib_count
 
@@ -513,22 +560,21 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
          isect_offsets, flatten_ids, render_colors, render_alphas, last_ids, median_ids,
          gaussian_ids) = ctx.saved_tensors
         (range_x, range_y, width, height, tile_size, absgrad, g_weight, adjoint, bg_grad_index_ok,
-         gs_contrib_threshold, N, n_contrib) = ctx.cfg
+         gs_contrib_threshold, N, n_contrib, C, pshape) = ctx.cfg
         dev = means2d.device
-        C = isect_offsets.shape[0]
         D = colors.shape[-1]
 
         def g(t, shape):
             return torch.zeros(shape, dtype=torch.float32, device=dev) if t is None else t.float().contiguous()
 
-        v_rc = g(v_render_colors, (C, height, width, D))
-        v_ra = g(v_render_alphas, (C, height, width, 1))
-        v_rn = g(v_render_normals, (C, height, width, 3))
-        v_rd = g(v_render_distort, (C, height, width, 1))
-        v_rm = g(v_render_median, (C, height, width, 1))
+        v_rc = g(v_render_colors, pshape + (D,))
+        v_ra = g(v_render_alphas, pshape + (1,))
+        v_rn = g(v_render_normals, pshape + (3,))
+        v_rd = g(v_render_distort, pshape + (1,))
+        v_rm = g(v_render_median, pshape + (1,))
         f = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
                       backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-                      0.0, g_weight, C, N)
+                      0.0, g_weight, C, N, ctx.layout)
         v_means2d = torch.empty_like(means2d)
         v_means2d_abs = torch.empty_like(means2d) if absgrad else None
         v_ray_transforms = torch.empty_like(ray_transforms)
@@ -549,16 +595,30 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
             means2d.absgrad = v_means2d_abs
         v_backgrounds = None
         if bg_grad_index_ok and backgrounds is not None and ctx.needs_input_grad[7]:
-            v_backgrounds = (v_rc * (1.0 - render_alphas).float()).sum(dim=(1, 2))
+            if len(pshape) == 3:
+                v_backgrounds = (v_rc * (1.0 - render_alphas).float()).sum(dim=(1, 2))
+            else:
+                vt = ctx.layout["view_table"]
+                v_backgrounds = torch.stack([(v_rc[b:b + n] * (1.0 - render_alphas[b:b + n])).sum(0)
+                                             for b, n in zip(vt.pix_base, vt.pix_count)])
         if v_textures is not None and textures.dtype != torch.float32:
             v_textures = v_textures.to(textures.dtype)
         return (v_means2d, v_ray_transforms, v_colors, v_opacities, v_textures, v_normals, v_densify, v_backgrounds,
-                None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None)
+                None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None,
+                None)
+
+
+def _layout(tile_order, view_table):
+    if tile_order is None and view_table is None:
+        return None
+    if tile_order is not None:
+        tile_order = tile_order.to(torch.int32).contiguous()
+    return {"tile_order": tile_order, "view_table": view_table}
 
 
 def _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
-                  backgrounds, packed):
-    C = isect_offsets.size(0)
+                  backgrounds, packed, view_table=None):
+    C = isect_offsets.size(0) if view_table is None else view_table.n_views
     if packed:
         nnz = means2d.size(0)
         assert means2d.shape == (nnz, 2), means2d.shape
@@ -573,6 +633,11 @@ def _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, til
         assert opacities.shape == (C, N), opacities.shape
     if backgrounds is not None:
         assert backgrounds.shape == (C, colors.shape[-1]), backgrounds.shape
+    if view_table is not None:
+        assert packed, "the batching form takes packed inputs"
+        assert isect_offsets.shape == (view_table.n_tiles,), isect_offsets.shape
+        assert tile_size == view_table.tile_size, (tile_size, view_table.tile_size)
+        return
     tile_height, tile_width = isect_offsets.shape[1:3]
     assert tile_height * tile_size >= image_height, f"Assert Failed: {tile_height} * {tile_size} >= {image_height}"
     assert tile_width * tile_size >= image_width, f"Assert Failed: {tile_width} * {tile_size} >= {image_width}"
@@ -605,6 +670,8 @@ def rasterize_to_pixels_textured_gaussians(
     texture_storage: Optional[Tensor] = None,
     texture_scales: Optional[Tensor] = None,
     gaussian_ids: Optional[Tensor] = None,
+    tile_order: Optional[Tensor] = None,
+    view_table=None,
 ) -> Tuple[Tensor, ...]:
     """Rasterize textured 2D Gaussians to pixels (reference: cuda/_wrapper.py:1806-2002).
 
@@ -619,9 +686,15 @@ def rasterize_to_pixels_textured_gaussians(
     the contribution statistics are per Gaussian, [N].  The reference indexes
     textures and statistics with the packed entry index, out of range for
     packed inputs, so it is not followed there.
+
+    ``tile_order`` (a permutation of the tiles, e.g. from
+    :func:`tile_order_heaviest_first`) sets the order in which tiles are
+    taken; ``view_table`` selects the batching form (views of uneven size,
+    flat ``isect_offsets`` from :func:`isect_offset_encode_views`, flat
+    per-pixel outputs [n_pixels, ...]).
     """
     _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
-                  backgrounds, packed)
+                  backgrounds, packed, view_table)
     if filtering not in _FILTER_ADJOINT:
         raise Exception(f"Unsupported filter type {filtering}")
     assert textures.dim() == 4 and textures.shape[-1] == 4, textures.shape
@@ -646,7 +719,7 @@ def rasterize_to_pixels_textured_gaussians(
         None if backgrounds is None else backgrounds.contiguous(), masks, store, texture_scales,
         float(texture_range_x), float(texture_range_y), int(image_width), int(image_height), int(tile_size),
         isect_offsets.contiguous(), flatten_ids.contiguous(), absgrad, gs_contrib_threshold, g_weight,
-        _FILTER_ADJOINT[filtering], False, gaussian_ids, textures.shape[0])
+        _FILTER_ADJOINT[filtering], False, gaussian_ids, textures.shape[0], _layout(tile_order, view_table))
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]
@@ -674,6 +747,8 @@ def rasterize_to_pixels_2dgs(
     *,
     gaussian_ids: Optional[Tensor] = None,
     n_gaussians: Optional[int] = None,
+    tile_order: Optional[Tensor] = None,
+    view_table=None,
 ) -> Tuple[Tensor, ...]:
     """Rasterize plain 2D Gaussians to pixels (reference: cuda/_wrapper.py:1647-1784).
 
@@ -681,10 +756,11 @@ def rasterize_to_pixels_2dgs(
     when the backgrounds require it (reference: cuda/_wrapper.py:2920-2925).
     Packed inputs: the contribution statistics are per entry, [nnz], or per
     Gaussian, [n_gaussians], when ``gaussian_ids`` and ``n_gaussians`` are
-    given (the reference sizes them [0] for packed inputs).
+    given (the reference sizes them [0] for packed inputs).  ``tile_order`` and
+    ``view_table`` as in :func:`rasterize_to_pixels_textured_gaussians`.
     """
     _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
-                  backgrounds, packed)
+                  backgrounds, packed, view_table)
     if packed and gaussian_ids is not None:
         if n_gaussians is None:
             raise ValueError("gaussian_ids needs n_gaussians")
@@ -699,7 +775,7 @@ def rasterize_to_pixels_2dgs(
         normals.contiguous(), densify.contiguous(), None if backgrounds is None else backgrounds.contiguous(), masks,
         None, None, 3.0, 3.0, int(image_width), int(image_height), int(tile_size), isect_offsets.contiguous(),
         flatten_ids.contiguous(), absgrad, gs_contrib_threshold, 1.0, B.TG_ADJ_REFERENCE, True, gaussian_ids,
-        int(n_gaussians))
+        int(n_gaussians), _layout(tile_order, view_table))
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]

@@ -15,7 +15,9 @@ entries only, ``meta["camera_ids"]`` / ``meta["gaussian_ids"]``), with
 Extensions (keyword-only, default off): ``texture_storage`` /
 ``texture_scales`` (sample BF16 / FP16 / FP8 textures, gradients to the FP32
 ``textures``), ``filtering="bilinear_exact"`` and ``adjoint="exact"`` (exact
-adjoint end to end).
+adjoint end to end), ``tile_order`` ("heaviest_first", the default: compositor
+tiles taken by descending intersection count, so the longest tiles do not form
+the launch's tail; "launch": tile index order; the results are the same).
 """
 from __future__ import annotations
 
@@ -29,6 +31,7 @@ from .cuda._wrapper import (
     fully_fused_projection_2dgs,
     isect_offset_encode,
     isect_tiles,
+    tile_order_heaviest_first,
     rasterize_to_pixels_2dgs,
     rasterize_to_pixels_textured_gaussians,
     spherical_harmonics,
@@ -41,7 +44,8 @@ _RENDER_MODES = ["RGB", "D", "ED", "RGB+D", "RGB+ED"]
 
 def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, height, near_plane, far_plane,
              radius_clip, eps2d, sh_degree, packed, tile_size, render_mode, sparse_grad, norm_rot_grad, distloss,
-             adjoint):
+             adjoint, tile_order="heaviest_first"):
+    assert tile_order in ("launch", "heaviest_first"), tile_order
     N = means.shape[0]
     C = viewmats.shape[0]
     assert means.shape == (N, 3), means.shape
@@ -79,6 +83,7 @@ def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, heigh
         means2d, radii, depths, tile_size, tile_width, tile_height, packed=packed, n_cameras=C,
         camera_ids=camera_ids, gaussian_ids=gaussian_ids)
     isect_offsets = isect_offset_encode(isect_ids, C, tile_width, tile_height)
+    order = tile_order_heaviest_first(isect_offsets, flatten_ids.numel()) if tile_order == "heaviest_first" else None
 
     if sh_degree is not None:
         camtoworlds = torch.inverse(viewmats)
@@ -102,7 +107,7 @@ def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, heigh
     return dict(C=C, radii=radii, means2d=means2d, depths=depths, ray_transforms=ray_transforms, normals=normals,
                 opacities=opacities, colors=colors, densify=densify, tile_width=tile_width, tile_height=tile_height,
                 tiles_per_gauss=tiles_per_gauss, isect_ids=isect_ids, flatten_ids=flatten_ids,
-                isect_offsets=isect_offsets, camera_ids=camera_ids, gaussian_ids=gaussian_ids)
+                isect_offsets=isect_offsets, camera_ids=camera_ids, gaussian_ids=gaussian_ids, tile_order=order)
 
 
 def _finish(p, render_colors, render_alphas, render_normals, render_distort, render_median, gs_contrib_sum,
@@ -168,6 +173,7 @@ def rasterization_2dgs(
     gs_contrib_threshold: float = 0.0,
     *,
     adjoint: str = "reference",
+    tile_order: str = "heaviest_first",
 ) -> Tuple[Tensor, Tensor, Tensor, Optional[Tensor], Tensor, Tensor, Tensor, Tensor, Dict]:
     """Rasterize 2D Gaussian surfels (N) to C image planes (reference: rendering.py:1009-1338).
 
@@ -177,12 +183,12 @@ def rasterization_2dgs(
     """
     p = _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, height, near_plane, far_plane,
                  radius_clip, eps2d, sh_degree, packed, tile_size, render_mode, sparse_grad, norm_rot_grad, distloss,
-                 adjoint)
+                 adjoint, tile_order)
     outs = rasterize_to_pixels_2dgs(
         p["means2d"], p["ray_transforms"], p["colors"], p["opacities"], p["normals"], p["densify"], width, height,
         tile_size, p["isect_offsets"], p["flatten_ids"], backgrounds=backgrounds, packed=packed, absgrad=absgrad,
         distloss=distloss, gs_contrib_threshold=gs_contrib_threshold, gaussian_ids=p["gaussian_ids"],
-        n_gaussians=means.shape[0] if packed else None)
+        n_gaussians=means.shape[0] if packed else None, tile_order=p["tile_order"])
     return _finish(p, *outs, viewmats, Ks, width, height, tile_size, render_mode, depth_mode)
 
 
@@ -220,6 +226,7 @@ def rasterization_textured_gaussians(
     texture_storage: Optional[Tensor] = None,
     texture_scales: Optional[Tensor] = None,
     adjoint: str = "reference",
+    tile_order: str = "heaviest_first",
 ) -> Tuple[Tensor, Tensor, Tensor, Optional[Tensor], Tensor, Tensor, Tensor, Tensor, Dict]:
     """Rasterize textured 2D Gaussian surfels (reference: rendering.py:1342-1685).
 
@@ -231,11 +238,12 @@ def rasterization_textured_gaussians(
     assert textures.shape[0] == N and textures.shape[-1] == 4 and textures.dim() == 4, textures.shape
     p = _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, height, near_plane, far_plane,
                  radius_clip, eps2d, sh_degree, packed, tile_size, render_mode, sparse_grad, norm_rot_grad, distloss,
-                 adjoint)
+                 adjoint, tile_order)
     outs = rasterize_to_pixels_textured_gaussians(
         p["means2d"], p["ray_transforms"], p["colors"], p["opacities"], textures, texture_range_x, texture_range_y,
         p["normals"], p["densify"], width, height, tile_size, p["isect_offsets"], p["flatten_ids"],
         backgrounds=backgrounds, packed=packed, absgrad=absgrad, distloss=distloss,
         gs_contrib_threshold=gs_contrib_threshold, filtering=filtering, g_weight=g_weight,
-        texture_storage=texture_storage, texture_scales=texture_scales, gaussian_ids=p["gaussian_ids"])
+        texture_storage=texture_storage, texture_scales=texture_scales, gaussian_ids=p["gaussian_ids"],
+        tile_order=p["tile_order"])
     return _finish(p, *outs, viewmats, Ks, width, height, tile_size, render_mode, depth_mode)
