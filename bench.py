@@ -276,7 +276,11 @@ def _run_ours(args, rank, world, local, dev):
     with ClockSampler(local) as clk:
         total_bf16, per_bf16, stages_bf16, launches, out = timed(store, tile, False, args.steps, args.warmup)
     total_bf16 = max_over_ranks(total_bf16, world)
-    meta = out[-1]
+    fwd_b, bwd_b, counts = compositor_bytes(out[-1], 3, R, 2, N, C, H, W)
+    del out  # no live autograd graph may reach the leaves when a CUDA graph is captured
+    graphed = None
+    if not args.no_graph:
+        graphed = time_graphed(lambda: step(store, tile, False), args.steps, C * H * W * world)
     # FP32 plain drop-in on the same GPU: FP32 textures, one camera per call, tile 16
     total_f32, per_f32, stages_f32, launches_f32, _ = timed(None, 16, True, args.steps, args.warmup)
     total_f32 = max_over_ranks(total_f32, world)
@@ -287,7 +291,6 @@ def _run_ours(args, rank, world, local, dev):
 
     # roofline of the dominant kernel (the compositor adjoint call)
     peaks, peaks_kind = load_peaks()
-    fwd_b, bwd_b, counts = compositor_bytes(meta, 3, R, 2, N, C, H, W)
     bwd_ms = statistics.mean(stages_bf16["tg_rasterize_bwd"])
     achieved = bwd_b / (bwd_ms / 1e3) / 1e9
     roofline = {"kernel": "tg_rasterize_bwd (compositor adjoint: gradient zero-fill + adjoint kernel + densify)",
@@ -323,10 +326,36 @@ def _run_ours(args, rank, world, local, dev):
                        "stage_ms": stage_ms_f32},
         "bf16_over_fp32": round(value / value_f32, 3),
         "stage_ms": stage_ms, "per_step_ms": [round(x, 3) for x in per_bf16],
+        "graphed": graphed,
         "counts": counts, "roofline": roofline, "gpu_launches": int(launches),
         "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
+
+
+def time_graphed(fn, steps, pixels):
+    """The same step captured once in a CUDA graph (forward, loss and backward; intersection buffers sized by
+    capacity, no host synchronisation) and replayed `steps` times."""
+    import torch
+    from textured_gaussians_b200.graph import GraphedStep
+
+    g = GraphedStep(fn)
+    g.replay()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        g.replay()
+    t1.record()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / steps
+    over = g.overflowed()
+    out = {"value": round(pixels / (ms / 1e3) / 1e6, 2), "unit": "Mpix/s", "ms_per_step": round(ms, 3),
+           "capacities": g.capacities, "recorded_sizes": g.sizes, "overflowed": over}
+    del g
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_e2e(args, sc, tex32, store, w_rgb, w_a, dev, world):
@@ -562,6 +591,7 @@ def _run_batch(args, dev):
     with ClockSampler(0) as clk:
         ms_b, stages_b, launches_b = timed(lambda: step_batch(tile, "heaviest_first"), args.steps, args.warmup)
     ms_launch, _, _ = timed(lambda: step_batch(tile, "launch"), args.steps, 1)
+    graphed = None if args.no_graph else time_graphed(lambda: step_batch(tile, "heaviest_first"), args.steps, n_pix)
     ms_pv, stages_pv, launches_pv = timed(step_per_view, args.steps, 1)
     line = {
         "metric": "textured 2DGS fwd+bwd Mpix/s, batching form: 64 uneven views over 3 scenes in one call",
@@ -577,7 +607,7 @@ def _run_batch(args, dev):
         "per_view_fp32": {"value": round(n_pix / (ms_pv / 1e3) / 1e6, 2), "unit": "Mpix/s",
                           "ms_per_step": round(ms_pv, 3), "form": "FP32 plain drop-in, one call per view, tile 16",
                           "stage_ms": stages_pv, "gpu_launches": int(launches_pv)},
-        "batch_over_per_view_fp32": round(ms_pv / ms_b, 3),
+        "batch_over_per_view_fp32": round(ms_pv / ms_b, 3), "graphed": graphed,
         "stage_ms": stages_b, "gpu_launches": int(launches_b), "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -620,6 +650,7 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="tile size of the headline form (0 = autotune over 8, 16)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay timing")
     ap.add_argument("--workload", default="mixture1m", choices=["mixture1m", "batch"],
                     help="mixture1m: the headline workload; batch: 64 uneven views over 3 scenes (batching form)")
     ap.add_argument("--views", type=int, default=64, help="views of the batch workload")

@@ -155,6 +155,13 @@ typedef struct {
     const tg_view* views;         /* [C] or NULL */
     const int64_t* gauss_ranges;  /* [C,2] or NULL */
     int32_t max_range;
+    /* Capacity mode (overflow != NULL, for CUDA-graph capture): nnz_host is the
+     * capacity of the output arrays rather than *nnz; emit zeroes all of them
+     * (radii 0: the unused tail intersects nothing; its Gaussian ids are spread
+     * over [0, N) so gathers over the tail do not collide), writes the first
+     * min(*nnz, capacity) entries and sets *overflow to 1 if *nnz > capacity.
+     * The caller zeroes *overflow. */
+    uint32_t* overflow;
 } tg_project_packed_args;
 TG_API size_t tg_project_packed_workspace_bytes(int32_t C, int32_t N);
 TG_API int tg_project_packed_count(const tg_project_packed_args* a, tg_stream_t stream);
@@ -213,6 +220,14 @@ typedef struct {
      * then the largest grid's, which sets the tile bits of the keys); tile ids
      * in the keys are local to the camera.  NULL: one grid for all cameras. */
     const tg_view* views;       /* [n_cameras] or NULL */
+    /* Capacity mode (overflow != NULL; for CUDA-graph capture, where the count
+     * cannot be read back between the two calls): isect_ids / flatten_ids hold
+     * `capacity` entries, emit writes the first min(*n_isects, capacity),
+     * sets *overflow to 1 if *n_isects > capacity, and fills the rest of the
+     * keys with 2^(32+tile_bits+camera_bits) - 1, which sorts after every real
+     * key.  The caller zeroes *overflow. */
+    int64_t capacity;
+    uint32_t* overflow;
 } tg_isect_args;
 TG_API size_t tg_scan_workspace_bytes(int64_t n_elems);
 TG_API int tg_isect_count(const tg_isect_args* a, tg_stream_t stream);
@@ -237,6 +252,22 @@ TG_API int tg_sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_
  * Calls share that array: those that overlap on one GPU race and must be
  * serialised by the caller.  The first call on a device looks up the array's
  * address with that device current; make it before any stream capture. */
+/* Waits for `stream`, then reports whether any bounded look-back wait of the
+ * last tg_sort_pairs call that used `workspace` (with the same n and end_bit)
+ * gave up: TG_ERR_TIMEOUT if so, TG_OK otherwise.  Synchronising; for
+ * diagnostics and tests.  No counterpart in the reference. */
+TG_API int tg_sort_status(const void* workspace, int64_t n, int32_t end_bit, tg_stream_t stream);
+
+/* Diagnostic self-test of the sort's bounded waits (no counterpart in the
+ * reference): one pass over 8192 pairs (8 key bits) of keys/vals into
+ * keys_alt/vals_alt, run by a single CTA that is made to wait for a
+ * predecessor tile that never publishes.  The wait gives up after its poll
+ * limit (about a second), raises the error flag and the kernel returns; the
+ * call then synchronises and returns TG_ERR_TIMEOUT -- the expected outcome --
+ * with the CUDA context still usable.  workspace: tg_sort_workspace_bytes(8192, 8). */
+TG_API int tg_sort_lookback_selftest(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt,
+                                     void* workspace, size_t workspace_bytes, tg_stream_t stream);
+
 #define TG_SORT_NOALLOC_MAX_PAIRS 4194304
 TG_API int tg_sort_pairs_noalloc(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, int64_t n,
                                  int32_t end_bit, int32_t* result_in_alt, tg_stream_t stream);
@@ -303,6 +334,9 @@ typedef struct {
     const tg_view* views;
     const int32_t* tile_view;
     int64_t n_tiles, n_pixels;
+    /* Capacity mode: device count of valid intersections (flatten_ids then
+     * holds n_isects >= *n_isects_dev entries, the tail unused), or NULL. */
+    const int64_t* n_isects_dev;
 } tg_raster_fwd_args;
 TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
 

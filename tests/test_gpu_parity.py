@@ -337,3 +337,24 @@ def test_end_to_end_small_matches_oracle_pipeline():
                   ("textures", tex)]:
         assert rel_l2(to_np(t.grad), g[nm]) < 1e-4, (nm, rel_l2(to_np(t.grad), g[nm]))
         assert cosine(to_np(t.grad), g[nm]) > 0.99999
+
+
+def test_sort_bounded_wait_gives_up_with_a_status_and_the_context_survives():
+    """Failure detection without a fault: a look-back wait that nothing will
+    satisfy gives up after its poll limit, the call returns TG_ERR_TIMEOUT,
+    and the next sort on the same context is correct (and reports OK)."""
+    from textured_gaussians_b200 import _backend as B
+
+    L = B.lib()
+    n = 8192
+    keys = torch.randint(0, 1 << 40, (n,), dtype=torch.int64, device=DEV)
+    vals = torch.arange(n, dtype=torch.int32, device=DEV)
+    ka, va = torch.empty_like(keys), torch.empty_like(vals)
+    wsb = L.tg_sort_workspace_bytes(n, 8)
+    ws = torch.empty((wsb,), dtype=torch.uint8, device=DEV)
+    st = torch.cuda.current_stream().cuda_stream
+    rc = L.tg_sort_lookback_selftest(B.ptr(keys), B.ptr(vals), B.ptr(ka), B.ptr(va), B.ptr(ws), wsb, st)
+    assert rc == -5, (rc, L.tg_last_error())
+    k2, v2 = sort_pairs(keys.clone(), vals.clone(), 40, check=True)
+    ref = torch.sort(keys, stable=True)
+    assert torch.equal(k2, ref.values) and torch.equal(v2.long(), ref.indices)

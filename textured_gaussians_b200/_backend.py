@@ -43,7 +43,7 @@ class ProjectPackedArgs(ctypes.Structure):
                 ("width", I32), ("height", I32), ("near_plane", F32), ("far_plane", F32), ("radius_clip", F32),
                 ("workspace", P), ("nnz", P), ("indptr", P), ("nnz_host", I64), ("camera_ids", P),
                 ("gaussian_ids", P), ("radii", P), ("means2d", P), ("depths", P), ("ray_transforms", P),
-                ("normals", P), ("views", P), ("gauss_ranges", P), ("max_range", I32)]
+                ("normals", P), ("views", P), ("gauss_ranges", P), ("max_range", I32), ("overflow", P)]
 
 
 class ProjectPackedBwdArgs(ctypes.Structure):
@@ -57,7 +57,7 @@ class IsectArgs(ctypes.Structure):
     _fields_ = [("n_elems", I64), ("N", I64), ("camera_ids", P), ("means2d", P), ("radii", P), ("depths", P),
                 ("tile_size", I32), ("tile_width", I32), ("tile_height", I32), ("n_cameras", I32),
                 ("tiles_per_gauss", P), ("cum_tiles", P), ("n_isects", P), ("scan_workspace", P),
-                ("isect_ids", P), ("flatten_ids", P), ("views", P)]
+                ("isect_ids", P), ("flatten_ids", P), ("views", P), ("capacity", I64), ("overflow", P)]
 
 
 class RasterFwdArgs(ctypes.Structure):
@@ -69,7 +69,7 @@ class RasterFwdArgs(ctypes.Structure):
                 ("gaussian_ids", P), ("contrib_threshold", F32), ("g_weight", F32), ("n_contrib", I32),
                 ("out_colors", P), ("out_alphas", P), ("out_normals", P), ("out_distort", P), ("out_median", P),
                 ("last_ids", P), ("median_ids", P), ("contrib_sum", P), ("contrib_count", P), ("tile_order", P),
-                ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64)]
+                ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64), ("n_isects_dev", P)]
 
 
 class RasterBwdArgs(ctypes.Structure):
@@ -107,6 +107,8 @@ def lib() -> ctypes.CDLL:
                 ("tg_isect_count", [ctypes.POINTER(IsectArgs), P]),
                 ("tg_isect_emit", [ctypes.POINTER(IsectArgs), P]),
                 ("tg_sort_pairs", [P, P, P, P, I64, I32, P, ctypes.c_size_t, ctypes.POINTER(I32), P]),
+                ("tg_sort_status", [P, I64, I32, P]),
+                ("tg_sort_lookback_selftest", [P, P, P, P, P, ctypes.c_size_t, P]),
                 ("tg_isect_offset_encode", [P, I64, I32, I32, I32, P, P]),
                 ("tg_isect_offset_encode_views", [P, I64, I32, I64, P, P, I64, P, P]),
                 ("tg_rasterize_fwd", [ctypes.POINTER(RasterFwdArgs), P]),

@@ -36,11 +36,13 @@ from .cuda._wrapper import (
     _FullyFusedProjectionPacked2DGS,
     isect_offset_encode_views,
     isect_tiles,
+    n_isects_of,
     rasterize_to_pixels_2dgs,
     rasterize_to_pixels_textured_gaussians,
     spherical_harmonics,
     tile_order_heaviest_first,
 )
+from .rendering import _inverse
 from .utils import depth_to_normal
 
 # layout of tg_view (include/tg2dgs.h)
@@ -72,8 +74,21 @@ class ViewTable:
         arr["width"], arr["height"] = self.widths, self.heights
         arr["tile_width"], arr["tile_height"] = self.tile_w, self.tile_h
         arr["tile_base"], arr["pix_base"] = self.tile_base, self.pix_base
+        self.device = device
         self.views = torch.from_numpy(arr.view(np.uint8).copy()).to(device)
         self.tile_view = torch.from_numpy(np.repeat(np.arange(self.n_views, dtype=np.int32), tiles)).to(device)
+        self._ranges = {}
+
+    def gauss_ranges(self, scene_offsets: Sequence[int], view_scenes: Sequence[int]):
+        """[C,2] int64 device tensor of each view's Gaussian range, and the longest
+        range (cached, so a captured step makes no host-to-device copy)."""
+        key = (tuple(int(o) for o in scene_offsets), tuple(int(v) for v in view_scenes))
+        if key not in self._ranges:
+            offs = key[0]
+            rng = [(offs[v], offs[v + 1]) for v in key[1]]
+            t = torch.tensor(rng, dtype=torch.int64).to(self.device)
+            self._ranges[key] = (t, max(b - a for a, b in rng))
+        return self._ranges[key]
 
     def split(self, flat: Tensor) -> List[Tensor]:
         """Per-view [H, W, ...] views of a flat per-pixel tensor [n_pixels, ...]."""
@@ -141,9 +156,7 @@ def rasterization_textured_gaussians_batch(
     vt = view_table or ViewTable(widths, heights, tile_size, dev)
     assert vt.widths == [int(w) for w in widths] and vt.heights == [int(h) for h in heights]
     assert vt.tile_size == tile_size
-    ranges_h = [(offs[s], offs[s + 1]) for s in view_scenes]
-    ranges = torch.tensor(ranges_h, dtype=torch.int64, device=dev)
-    max_range = max(b - a for a, b in ranges_h)
+    ranges, max_range = vt.gauss_ranges(offs, view_scenes)
     mode = B.TG_ADJ_EXACT if adjoint == "exact" else (B.TG_ADJ_BWD2 if norm_rot_grad else B.TG_ADJ_REFERENCE)
 
     camera_ids, gaussian_ids, radii, means2d, depths, ray_transforms, normals = _FullyFusedProjectionPacked2DGS.apply(
@@ -151,7 +164,7 @@ def rasterization_textured_gaussians_batch(
         eps2d, near_plane, far_plane, radius_clip, False, mode, (vt.views, ranges, max_range))
     opac = opacities[gaussian_ids]
     if sh_degree is not None:
-        camtoworlds = torch.inverse(viewmats)
+        camtoworlds = _inverse(viewmats)
         dirs = means[gaussian_ids, :] - camtoworlds[camera_ids, :3, 3]
         cols = spherical_harmonics(sh_degree, dirs, colors[gaussian_ids], masks=radii > 0)
         cols = torch.clamp_min(cols + 0.5, 0.0)
@@ -167,7 +180,8 @@ def rasterization_textured_gaussians_batch(
         means2d, radii, depths, tile_size, 0, 0, packed=True, n_cameras=C, camera_ids=camera_ids,
         gaussian_ids=gaussian_ids, view_table=vt)
     isect_offsets = isect_offset_encode_views(isect_ids, vt)
-    order = tile_order_heaviest_first(isect_offsets, flatten_ids.numel()) if tile_order == "heaviest_first" else None
+    order = (tile_order_heaviest_first(isect_offsets, n_isects_of(flatten_ids)) if tile_order == "heaviest_first"
+             else None)
 
     common = dict(backgrounds=backgrounds, packed=True, absgrad=absgrad, gs_contrib_threshold=gs_contrib_threshold,
                   gaussian_ids=gaussian_ids, tile_order=order, view_table=vt)
@@ -185,7 +199,7 @@ def rasterization_textured_gaussians_batch(
     if render_mode in ("ED", "RGB+ED"):
         flat_colors = torch.cat([flat_colors[..., :-1], flat_colors[..., -1:] / flat_alphas.clamp(min=1e-10)], dim=-1)
 
-    camtoworlds = torch.linalg.inv(viewmats)
+    camtoworlds = _inverse(viewmats)
     colors_v, alphas_v = vt.split(flat_colors), vt.split(flat_alphas)
     median_v = vt.split(flat_median)
     normals_v = [torch.einsum("ij,hwj->hwi", camtoworlds[c, :3, :3], n)

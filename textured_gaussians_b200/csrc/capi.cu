@@ -21,7 +21,10 @@ cudaError_t launch_project_packed_emit(const tg_project_packed_args& a, cudaStre
 cudaError_t launch_project_packed_bwd(const tg_project_packed_bwd_args& a, cudaStream_t s);
 size_t scan_workspace_bytes(int64_t n_elems);
 cudaError_t launch_isect_count(const tg_isect_args& a, cudaStream_t s);
-cudaError_t launch_isect_emit(const tg_isect_args& a, int tile_n_bits, cudaStream_t s);
+cudaError_t launch_isect_emit(const tg_isect_args& a, int tile_n_bits, int end_bit, cudaStream_t s);
+uint32_t* sort_error_flag(void* workspace, int64_t n, int end_bit);
+int sort_lookback_selftest(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, void* workspace,
+                           size_t ws_bytes, cudaStream_t s, cudaError_t& cerr);
 size_t sort_workspace_bytes(int64_t n, int end_bit);
 int sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, int64_t n, int end_bit,
                void* workspace, size_t ws_bytes, int32_t* result_in_alt, cudaStream_t s, cudaError_t& cerr);
@@ -196,6 +199,16 @@ int tg_project_packed_emit(const tg_project_packed_args* a, tg_stream_t stream) 
                    a->normals,
                TG_ERR_INVALID_ARG, "null output pointer");
     TG_REQUIRE(aligned(a->means2d, 8), TG_ERR_INVALID_ARG, "means2d must be 8-byte aligned");
+    if (a->overflow) {  // capacity mode: every output zeroed, so the unused tail is inert
+        const size_t n = (size_t)a->nnz_host;
+        struct Z { void* p; size_t b; } zs[] = {{a->camera_ids, 8 * n}, {a->gaussian_ids, 8 * n}, {a->radii, 4 * n},
+                                                {a->means2d, 8 * n},    {a->depths, 4 * n},       {a->ray_transforms, 36 * n},
+                                                {a->normals, 12 * n}};
+        for (const Z& z : zs) {
+            const cudaError_t e = cudaMemsetAsync(z.p, 0, z.b, stream);
+            if (e != cudaSuccess) return cuda_status(e, "tg_project_packed_emit memset");
+        }
+    }
     return cuda_status(tg::launch_project_packed_emit(*a, stream), "tg_project_packed_emit");
 }
 
@@ -239,12 +252,44 @@ int tg_isect_count(const tg_isect_args* a, tg_stream_t stream) {
 
 int tg_isect_emit(const tg_isect_args* a, tg_stream_t stream) {
     TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
-    if (a->n_elems == 0) return TG_OK;
-    TG_REQUIRE(a->means2d && a->radii && a->depths && a->cum_tiles && a->isect_ids && a->flatten_ids,
-               TG_ERR_INVALID_ARG, "null pointer");
-    TG_REQUIRE(a->camera_ids != nullptr || a->N > 0, TG_ERR_INVALID_ARG, "dense layout needs N > 0");
+    if (a->overflow) {
+        TG_REQUIRE(a->capacity >= 0 && a->capacity < (int64_t(1) << 31), TG_ERR_INVALID_ARG, "bad capacity");
+        TG_REQUIRE(a->n_isects && (a->capacity == 0 || (a->isect_ids && a->flatten_ids)), TG_ERR_INVALID_ARG,
+                   "capacity mode needs n_isects and the key / id buffers");
+    }
+    if (a->n_elems == 0 && !(a->overflow && a->capacity > 0)) return TG_OK;
+    if (a->n_elems > 0) {
+        TG_REQUIRE(a->means2d && a->radii && a->depths && a->cum_tiles && a->isect_ids && a->flatten_ids,
+                   TG_ERR_INVALID_ARG, "null pointer");
+        TG_REQUIRE(a->camera_ids != nullptr || a->N > 0, TG_ERR_INVALID_ARG, "dense layout needs N > 0");
+    }
     const int tb = bit_width((int64_t)a->tile_width * a->tile_height);
-    return cuda_status(tg::launch_isect_emit(*a, tb, stream), "tg_isect_emit");
+    const int cb = bit_width(a->n_cameras);
+    return cuda_status(tg::launch_isect_emit(*a, tb, 32 + tb + cb, stream), "tg_isect_emit");
+}
+
+int tg_sort_lookback_selftest(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, void* workspace,
+                              size_t workspace_bytes, tg_stream_t stream) {
+    TG_REQUIRE(keys && vals && keys_alt && vals_alt && workspace, TG_ERR_INVALID_ARG, "null pointer");
+    cudaError_t cerr;
+    const int rc = tg::sort_lookback_selftest(keys, vals, keys_alt, vals_alt, workspace, workspace_bytes, stream, cerr);
+    if (rc == TG_ERR_CUDA) return cuda_status(cerr, "tg_sort_lookback_selftest");
+    if (rc == TG_ERR_WORKSPACE) return fail(rc, "workspace smaller than tg_sort_workspace_bytes(8192, 8)");
+    if (rc == TG_ERR_TIMEOUT) return fail(rc, "look-back wait gave up (the expected outcome of this self-test)");
+    return rc;
+}
+
+int tg_sort_status(const void* workspace, int64_t n, int32_t end_bit, tg_stream_t stream) {
+    TG_REQUIRE(n >= 0 && end_bit >= 0 && end_bit <= 64, TG_ERR_INVALID_ARG, "bad sizes");
+    if (n <= 1 || end_bit == 0) return TG_OK;
+    TG_REQUIRE(workspace != nullptr, TG_ERR_INVALID_ARG, "null workspace");
+    const uint32_t* flag = tg::sort_error_flag(const_cast<void*>(workspace), n, end_bit);
+    uint32_t h = 0;
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaMemcpy(&h, flag, sizeof(h), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e, "tg_sort_status");
+    if (h) return fail(TG_ERR_TIMEOUT, "a look-back wait of the pair sort gave up");
+    return TG_OK;
 }
 
 size_t tg_sort_workspace_bytes(int64_t n, int32_t end_bit) { return tg::sort_workspace_bytes(n, end_bit); }

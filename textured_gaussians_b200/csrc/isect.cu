@@ -130,13 +130,26 @@ __global__ void __launch_bounds__(256) isect_emit_kernel(tg_isect_args a, int ti
     const int64_t cid_enc = cid << (32 + tile_n_bits);
     const int64_t depth_enc = (int64_t)__float_as_int(a.depths[e]);  // sign-extended like the reference
     int64_t cur = e == 0 ? 0 : a.cum_tiles[e - 1];
+    // capacity mode: only the first `capacity` entries exist
+    const int64_t limit = a.overflow ? a.capacity : INT64_MAX;
+    if (a.overflow && a.cum_tiles[e] > limit) atomicOr(a.overflow, 1u);
     for (uint32_t y = y0; y < y1; ++y)
         for (uint32_t x = x0; x < x1; ++x) {
+            if (cur >= limit) return;
             const int64_t tile_id = (int64_t)y * tw + x;
             a.isect_ids[cur] = cid_enc | (tile_id << 32) | depth_enc;
             a.flatten_ids[cur] = (int32_t)e;
             ++cur;
         }
+}
+
+// Capacity mode: keys past the valid count sort after every real key.
+__global__ void __launch_bounds__(256) isect_pad_kernel(int64_t* keys, int32_t* vals, const int64_t* n_dev,
+                                                        int64_t capacity, int64_t pad_key) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= capacity || i < *n_dev) return;
+    keys[i] = pad_key;
+    vals[i] = 0;
 }
 
 // offsets[t] = lower_bound over sorted keys of (camera, tile) index t.
@@ -398,13 +411,10 @@ int sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_al
     sort_digit_offsets_kernel<<<passes, kRadix, 0, s>>>(w.hist, w.digit_offsets);
     note_launches(2);
     if ((cerr = cudaGetLastError()) != cudaSuccess) return TG_ERR_CUDA;
-    static bool attr_set = false;  // benign race: every thread sets the same value
-    if (!attr_set) {
-        if ((cerr = cudaFuncSetAttribute(sort_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kSortSmem)) != cudaSuccess)
-            return TG_ERR_CUDA;
-        attr_set = true;
-    }
+    // a per-device function attribute: set on every call (cheap, allowed during stream capture)
+    if ((cerr = cudaFuncSetAttribute(sort_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kSortSmem)) != cudaSuccess)
+        return TG_ERR_CUDA;
     uint64_t* kin = reinterpret_cast<uint64_t*>(keys);
     uint32_t* vin = reinterpret_cast<uint32_t*>(vals);
     uint64_t* kout = reinterpret_cast<uint64_t*>(keys_alt);
@@ -423,6 +433,38 @@ int sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_al
     }
     *result_in_alt = passes & 1;
     return TG_OK;
+}
+
+__global__ void set_u32_kernel(uint32_t* p, uint32_t v) { *p = v; }
+
+// Diagnostic: one pass over two tiles (8192 pairs, 8 key bits) run by a single
+// CTA whose tile counter is preset to 1, so its look-back waits on tile 0,
+// which never publishes.  The bounded wait gives up after kSpinLimit polls and
+// raises the error flag; a partial prefix only lowers scatter positions, so
+// every write stays inside the output buffers.
+int sort_lookback_selftest(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, void* workspace,
+                           size_t ws_bytes, cudaStream_t s, cudaError_t& cerr) {
+    cerr = cudaSuccess;
+    constexpr int64_t n = 2 * kSortTile;
+    SortWorkspace w = carve_sort_workspace(workspace, n, 1);
+    if (ws_bytes < w.bytes) return TG_ERR_WORKSPACE;
+    if ((cerr = cudaMemsetAsync(workspace, 0, w.bytes, s)) != cudaSuccess) return TG_ERR_CUDA;
+    set_u32_kernel<<<1, 1, 0, s>>>(w.tile_counter, 1u);  // the single CTA takes tile 1
+    sort_histogram_kernel<<<2, kSortThreads, 0, s>>>(reinterpret_cast<const uint64_t*>(keys), n, 1, 8, w.hist);
+    sort_digit_offsets_kernel<<<1, kRadix, 0, s>>>(w.hist, w.digit_offsets);
+    if ((cerr = cudaFuncSetAttribute(sort_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kSortSmem)) != cudaSuccess)
+        return TG_ERR_CUDA;
+    sort_pass_kernel<<<1, kSortThreads, kSortSmem, s>>>(
+        reinterpret_cast<const uint64_t*>(keys), reinterpret_cast<const uint32_t*>(vals),
+        reinterpret_cast<uint64_t*>(keys_alt), reinterpret_cast<uint32_t*>(vals_alt), n, 0, 0xffu, w.digit_offsets,
+        w.status, w.tile_counter, w.error);
+    note_launches(4);
+    if ((cerr = cudaGetLastError()) != cudaSuccess) return TG_ERR_CUDA;
+    uint32_t h = 0;
+    if ((cerr = cudaStreamSynchronize(s)) != cudaSuccess) return TG_ERR_CUDA;
+    if ((cerr = cudaMemcpy(&h, w.error, sizeof(h), cudaMemcpyDeviceToHost)) != cudaSuccess) return TG_ERR_CUDA;
+    return h ? TG_ERR_TIMEOUT : TG_OK;
 }
 
 // error flag location inside a carved workspace (for the host to read back)
@@ -446,10 +488,17 @@ cudaError_t launch_isect_count(const tg_isect_args& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_isect_emit(const tg_isect_args& a, int tile_n_bits, cudaStream_t s) {
-    if (a.n_elems == 0) return cudaSuccess;
-    isect_emit_kernel<<<(unsigned)((a.n_elems + 255) / 256), 256, 0, s>>>(a, tile_n_bits);
-    note_launches(1);
+cudaError_t launch_isect_emit(const tg_isect_args& a, int tile_n_bits, int end_bit, cudaStream_t s) {
+    if (a.n_elems > 0) {
+        isect_emit_kernel<<<(unsigned)((a.n_elems + 255) / 256), 256, 0, s>>>(a, tile_n_bits);
+        note_launches(1);
+    }
+    if (a.overflow && a.capacity > 0) {
+        const int64_t pad = end_bit >= 63 ? INT64_MAX : (int64_t)((1ull << end_bit) - 1ull);
+        isect_pad_kernel<<<(unsigned)((a.capacity + 255) / 256), 256, 0, s>>>(a.isect_ids, a.flatten_ids, a.n_isects,
+                                                                              a.capacity, pad);
+        note_launches(1);
+    }
     return cudaGetLastError();
 }
 

@@ -206,10 +206,22 @@ __global__ void __launch_bounds__(kPackThreads) project_packed_emit_kernel(tg_pr
                 a.camera_ids[pos] = c;
                 a.gaussian_ids[pos] = n;
                 store_projected(o, pos, a.radii, a.means2d, a.depths, a.ray_transforms, a.normals);
+            } else if (a.overflow) {
+                atomicOr(a.overflow, 1u);
             }
         }
         run += slice_total;
     }
+}
+
+// Capacity mode: the unused tail [*nnz, capacity) keeps radius 0 (it intersects
+// nothing) and gets Gaussian ids spread over all N, so gathers and their
+// scatter-add adjoints over the tail do not pile onto one Gaussian.
+__global__ void __launch_bounds__(256) packed_tail_kernel(const int64_t* nnz, int64_t capacity, int32_t N,
+                                                          int64_t* gaussian_ids) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= capacity || i < *nnz) return;
+    gaussian_ids[i] = N > 0 ? i % N : 0;
 }
 
 // ------------------------------------------------------------------ adjoint
@@ -430,6 +442,11 @@ cudaError_t launch_project_packed_emit(const tg_project_packed_args& a, cudaStre
     project_packed_emit_kernel<<<dim3((unsigned)per_row, (unsigned)a.C), kPackThreads, 0, s>>>(
         a, static_cast<const int64_t*>(a.workspace));
     note_launches(1);
+    if (a.overflow) {
+        packed_tail_kernel<<<(unsigned)((a.nnz_host + 255) / 256), 256, 0, s>>>(a.nnz, a.nnz_host, a.N,
+                                                                                a.gaussian_ids);
+        note_launches(1);
+    }
     return cudaGetLastError();
 }
 

@@ -215,8 +215,10 @@ __device__ __forceinline__ TileWork tile_work(const tg_raster_fwd_args& a, int64
         w.pix_base = (int64_t)w.c * a.height * a.width;
         w.pix_limit = (int64_t)a.C * a.height * a.width;
     }
-    w.range_start = a.tile_offsets[w.t];
-    w.range_end = w.t == n_tiles - 1 ? (int32_t)a.n_isects : a.tile_offsets[w.t + 1];
+    // capacity mode: the valid intersections are the first *n_isects_dev of the n_isects entries
+    const int64_t n_valid = a.n_isects_dev ? min(max(*a.n_isects_dev, (int64_t)0), a.n_isects) : a.n_isects;
+    w.range_start = min(a.tile_offsets[w.t], (int32_t)n_valid);
+    w.range_end = w.t == n_tiles - 1 ? (int32_t)n_valid : min(a.tile_offsets[w.t + 1], (int32_t)n_valid);
     return w;
 }
 

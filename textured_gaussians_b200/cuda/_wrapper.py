@@ -30,6 +30,7 @@ import torch
 from torch import Tensor
 
 from .. import _backend as B
+from ..graph import active_plan
 
 _FILTER_ADJOINT = {
     "bilinear": B.TG_ADJ_REFERENCE,
@@ -247,7 +248,14 @@ class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
             a.views, a.gauss_ranges, a.max_range = B.ptr(batch[0]), B.ptr(batch[1]), int(batch[2])
         st = B.stream_of(means)
         B.call("tg_project_packed_count", st, B.lib().tg_project_packed_count, ctypes.byref(a), st)
-        nnz = int(nnz_dev.item())  # the one host synchronisation, as in the reference
+        plan = active_plan()
+        if plan is not None and plan.mode == "capture":  # no host read: capacity-sized outputs, overflow flag
+            nnz = plan.next_capacity()
+            a.overflow = B.ptr(plan.new_flag(dev))
+        else:
+            nnz = int(nnz_dev.item())  # the one host synchronisation, as in the reference
+            if plan is not None:
+                plan.sizes.append(nnz)
         camera_ids = torch.empty((nnz,), dtype=torch.int64, device=dev)
         gaussian_ids = torch.empty((nnz,), dtype=torch.int64, device=dev)
         radii = torch.empty((nnz,), dtype=torch.int32, device=dev)
@@ -362,7 +370,23 @@ def isect_tiles(
                     None if view_table is None else B.ptr(view_table.views))
     stream = B.stream_of(means2d)
     B.call("tg_isect_count", stream, B.lib().tg_isect_count, ctypes.byref(a), stream)
+    end_bit = 32 + _bit_width(tile_width * tile_height) + _bit_width(C)
+    plan = active_plan()
+    if plan is not None and plan.mode == "capture":
+        # no host read: capacity-sized keys (tail padded to sort last), device count attached to flatten_ids
+        cap = plan.next_capacity()
+        isect_ids = torch.empty((cap,), dtype=torch.int64, device=dev)
+        flatten_ids = torch.empty((cap,), dtype=torch.int32, device=dev)
+        a.isect_ids, a.flatten_ids = B.ptr(isect_ids), B.ptr(flatten_ids)
+        a.capacity, a.overflow = cap, B.ptr(plan.new_flag(dev))
+        B.call("tg_isect_emit", stream, B.lib().tg_isect_emit, ctypes.byref(a), stream)
+        if sort:
+            isect_ids, flatten_ids = sort_pairs(isect_ids, flatten_ids, end_bit)
+        flatten_ids._tg_n_isects = n_dev
+        return tiles_per_gauss, isect_ids, flatten_ids
     n_isects = int(n_dev.item())  # the one host synchronisation, as in the reference
+    if plan is not None:
+        plan.sizes.append(n_isects)
     isect_ids = torch.empty((n_isects,), dtype=torch.int64, device=dev)
     flatten_ids = torch.empty((n_isects,), dtype=torch.int32, device=dev)
     if n_isects:
@@ -370,13 +394,21 @@ def isect_tiles(
         a.flatten_ids = B.ptr(flatten_ids)
         B.call("tg_isect_emit", stream, B.lib().tg_isect_emit, ctypes.byref(a), stream)
         if sort:
-            end_bit = 32 + _bit_width(tile_width * tile_height) + _bit_width(C)
             isect_ids, flatten_ids = sort_pairs(isect_ids, flatten_ids, end_bit)
     return tiles_per_gauss, isect_ids, flatten_ids
 
 
-def sort_pairs(keys: Tensor, vals: Tensor, end_bit: int) -> Tuple[Tensor, Tensor]:
-    """Stable radix sort of (int64 key, int32 value) pairs on key bits [0, end_bit)."""
+def n_isects_of(flatten_ids: Tensor):
+    """Valid intersection count: a device tensor [1] for capacity-sized
+    intersections (graph capture), else the length of ``flatten_ids``."""
+    return getattr(flatten_ids, "_tg_n_isects", flatten_ids.numel())
+
+
+def sort_pairs(keys: Tensor, vals: Tensor, end_bit: int, check: bool = False) -> Tuple[Tensor, Tensor]:
+    """Stable radix sort of (int64 key, int32 value) pairs on key bits [0, end_bit).
+
+    ``check=True`` waits for the sort and raises if one of its bounded
+    look-back waits gave up (``tg_sort_status``)."""
     n = keys.numel()
     if n <= 1:
         return keys, vals
@@ -388,6 +420,8 @@ def sort_pairs(keys: Tensor, vals: Tensor, end_bit: int) -> Tuple[Tensor, Tensor
     st = B.stream_of(keys)
     B.call("tg_sort_pairs", st, B.lib().tg_sort_pairs, B.ptr(keys), B.ptr(vals), B.ptr(keys_alt), B.ptr(vals_alt), n,
            end_bit, B.ptr(ws), wsb, ctypes.byref(in_alt), st)
+    if check:
+        B.check(B.lib().tg_sort_status(B.ptr(ws), n, end_bit, st), "tg_sort_status")
     return (keys_alt, vals_alt) if in_alt.value else (keys, vals)
 
 
@@ -422,7 +456,11 @@ def tile_order_heaviest_first(isect_offsets: Tensor, n_isects: int) -> Tensor:
     so the longest tiles start first and the tail of the launch is short."""
     flat = isect_offsets.reshape(-1).to(torch.int64)
     n = flat.numel()
-    counts = torch.diff(flat, append=torch.tensor([n_isects], dtype=torch.int64, device=flat.device))
+    if isinstance(n_isects, Tensor):  # device count (graph capture)
+        tail = n_isects.reshape(1).to(torch.int64)
+    else:
+        tail = torch.full((1,), int(n_isects), dtype=torch.int64, device=flat.device)
+    counts = torch.diff(flat, append=tail)
     keys = ((1 << 31) - 1) - counts.clamp(0, (1 << 31) - 1)
     vals = torch.arange(n, dtype=torch.int32, device=flat.device)
     _, order = sort_pairs(keys.contiguous(), vals, 31)
@@ -483,7 +521,7 @@ def make_texture_storage(textures: Tensor, fmt: str) -> Tuple[Tensor, Optional[T
 
 def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_store, tex_scales, range_x, range_y,
               backgrounds, masks, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-              gs_contrib_threshold, g_weight, C, N, layout=None):
+              gs_contrib_threshold, g_weight, C, N, layout=None, n_isects_dev=None):
     D = colors.shape[-1]
     vt = None if layout is None else layout.get("view_table")
     th, tw = (1, 1) if vt is not None else isect_offsets.shape[1:3]
@@ -501,7 +539,7 @@ def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_stor
         int(n_contrib), None, None, None, None, None, None, None, None, None,
         None if layout is None else B.ptr(layout.get("tile_order")),
         None if vt is None else B.ptr(vt.views), None if vt is None else B.ptr(vt.tile_view),
-        0 if vt is None else vt.n_tiles, 0 if vt is None else vt.n_pixels)
+        0 if vt is None else vt.n_tiles, 0 if vt is None else vt.n_pixels, B.ptr(n_isects_dev))
 
 
 class _RasterizeToPixelsTextured(torch.autograd.Function):
@@ -526,9 +564,10 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         n_contrib = N if gaussian_ids is None else n_rows
         D = colors.shape[-1]
         m = None if masks is None else masks.to(torch.uint8).contiguous()
+        n_dev = getattr(flatten_ids, "_tg_n_isects", None)
         a = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
                       backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-                      gs_contrib_threshold, g_weight, C, N, layout)
+                      gs_contrib_threshold, g_weight, C, N, layout, n_dev)
         render_colors = torch.empty(pshape + (D,), dtype=torch.float32, device=dev)
         render_alphas = torch.empty(pshape + (1,), dtype=torch.float32, device=dev)
         render_normals = torch.empty(pshape + (3,), dtype=torch.float32, device=dev)
@@ -550,6 +589,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         ctx.cfg = (range_x, range_y, width, height, tile_size, absgrad, g_weight, adjoint, bg_grad_index_ok,
                    gs_contrib_threshold, N, n_contrib, C, pshape)
         ctx.layout = layout
+        ctx.n_isects_dev = n_dev
         ctx.mark_non_differentiable(contrib_sum, contrib_count)
         return render_colors, render_alphas, render_normals, render_distort, render_median, contrib_sum, contrib_count
 
@@ -574,7 +614,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         v_rm = g(v_render_median, pshape + (1,))
         f = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
                       backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-                      0.0, g_weight, C, N, ctx.layout)
+                      0.0, g_weight, C, N, ctx.layout, ctx.n_isects_dev)
         v_means2d = torch.empty_like(means2d)
         v_means2d_abs = torch.empty_like(means2d) if absgrad else None
         v_ray_transforms = torch.empty_like(ray_transforms)

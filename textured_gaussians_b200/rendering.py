@@ -31,6 +31,7 @@ from .cuda._wrapper import (
     fully_fused_projection_2dgs,
     isect_offset_encode,
     isect_tiles,
+    n_isects_of,
     tile_order_heaviest_first,
     rasterize_to_pixels_2dgs,
     rasterize_to_pixels_textured_gaussians,
@@ -40,6 +41,12 @@ from .cuda._wrapper import (
 from .utils import depth_to_normal
 
 _RENDER_MODES = ["RGB", "D", "ED", "RGB+D", "RGB+ED"]
+
+
+def _inverse(m: Tensor) -> Tensor:
+    """Batched 4x4 inverse without the host-side error check of torch.inverse
+    (the same kernel; no synchronisation, so it can sit inside a CUDA graph)."""
+    return torch.linalg.inv_ex(m)[0]
 
 
 def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, height, near_plane, far_plane,
@@ -83,10 +90,11 @@ def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, heigh
         means2d, radii, depths, tile_size, tile_width, tile_height, packed=packed, n_cameras=C,
         camera_ids=camera_ids, gaussian_ids=gaussian_ids)
     isect_offsets = isect_offset_encode(isect_ids, C, tile_width, tile_height)
-    order = tile_order_heaviest_first(isect_offsets, flatten_ids.numel()) if tile_order == "heaviest_first" else None
+    order = (tile_order_heaviest_first(isect_offsets, n_isects_of(flatten_ids)) if tile_order == "heaviest_first"
+             else None)
 
     if sh_degree is not None:
-        camtoworlds = torch.inverse(viewmats)
+        camtoworlds = _inverse(viewmats)
         if packed:
             dirs = means[gaussian_ids, :] - camtoworlds[camera_ids, :3, 3]
             colors = spherical_harmonics(sh_degree, dirs, colors[gaussian_ids], masks=radii > 0)  # [nnz, 3]
@@ -118,7 +126,7 @@ def _finish(p, render_colors, render_alphas, render_normals, render_distort, ren
             [render_colors[..., :-1], render_colors[..., -1:] / render_alphas.clamp(min=1e-10)], dim=-1)
     if render_mode in ["RGB+ED", "RGB+D"]:
         depth_for_normal = render_colors[..., -1:] if depth_mode == "expected" else render_median
-        render_normals_from_depth = depth_to_normal(depth_for_normal, torch.linalg.inv(viewmats), Ks).squeeze(0)
+        render_normals_from_depth = depth_to_normal(depth_for_normal, _inverse(viewmats), Ks).squeeze(0)
     meta = {
         "camera_ids": p["camera_ids"],
         "gaussian_ids": p["gaussian_ids"],
@@ -141,7 +149,7 @@ def _finish(p, render_colors, render_alphas, render_normals, render_distort, ren
         "render_distort": render_distort,
         "gradient_2dgs": p["densify"],
     }
-    render_normals = torch.einsum("...ij,...hwj->...hwi", torch.linalg.inv(viewmats)[..., :3, :3], render_normals)
+    render_normals = torch.einsum("...ij,...hwj->...hwi", _inverse(viewmats)[..., :3, :3], render_normals)
     return (render_colors, render_alphas, render_normals, render_normals_from_depth, render_distort, render_median,
             gs_contrib_sum, gs_contrib_count, meta)
 
