@@ -225,7 +225,7 @@ def _run_ours(args, rank, world, local, dev):
     w_rgb = torch.randn((C, H, W, 3), generator=g, device=dev)
     w_a = torch.randn((C, H, W, 1), generator=g, device=dev)
 
-    def step(storage, tile_size, per_view):
+    def step(storage, tile_size, per_view, depth=0):
         for t in (means, quats, scales, opac, colors, tex32):
             t.grad = None
         views = [slice(c, c + 1) for c in range(C)] if per_view else [slice(0, C)]
@@ -233,14 +233,14 @@ def _run_ours(args, rank, world, local, dev):
             out = rasterization_textured_gaussians(means, quats, scales, opac, colors, tex32, viewmats[v], Ks[v], W, H,
                                                    sh_degree=0, far_plane=100.0, tile_size=tile_size,
                                                    texture_storage=storage,
-                                                   tile_order=args.tile_order)
+                                                   tile_order=args.tile_order, batch_depth=depth)
             loss = (out[0] * w_rgb[v]).sum() + (out[1] * w_a[v]).sum()
             loss.backward()
         return out, loss
 
-    def timed(storage, tile_size, per_view, steps, warmup):
+    def timed(storage, tile_size, per_view, steps, warmup, depth=0):
         for _ in range(warmup):
-            step(storage, tile_size, per_view)
+            step(storage, tile_size, per_view, depth)
         torch.cuda.synchronize()
         barrier(world)
         torch.cuda.synchronize()
@@ -253,7 +253,7 @@ def _run_ours(args, rank, world, local, dev):
         t0.record()
         for i in range(steps):
             starts[i].record()
-            out, _ = step(storage, tile_size, per_view)
+            out, _ = step(storage, tile_size, per_view, depth)
             ends[i].record()
         t1.record()
         torch.cuda.synchronize()
@@ -265,22 +265,25 @@ def _run_ours(args, rank, world, local, dev):
         per = [a.elapsed_time(b) for a, b in zip(starts, ends)]
         return total_ms, per, stages, launches, out
 
-    # headline form: BF16 texture storage (FP32 master + gradients), all views in one call, tile size autotuned
-    from textured_gaussians_b200.tuning import autotune_tile_size
+    # headline form: BF16 texture storage (FP32 master + gradients), all views in one call, tile size and
+    # batch depth autotuned
+    from textured_gaussians_b200.tuning import autotune_compositor
 
     if args.tile:
-        tile, tune_ms = args.tile, {}
+        (tile, depth), tune_ms = (args.tile, args.depth), {}
     else:
-        tile, tune_ms = autotune_tile_size(("bench", N, C, W, H, R), lambda ts: step(store, ts, False))
-        tile = int(max_over_ranks(float(tile), world))  # every rank uses the same tile size
+        (tile, depth), tune_ms = autotune_compositor(("bench", N, C, W, H, R),
+                                                     lambda ts, d: step(store, ts, False, d))
+        tile = int(max_over_ranks(float(tile), world))  # every rank uses the same configuration
+        depth = int(max_over_ranks(float(depth), world))
     with ClockSampler(local) as clk:
-        total_bf16, per_bf16, stages_bf16, launches, out = timed(store, tile, False, args.steps, args.warmup)
+        total_bf16, per_bf16, stages_bf16, launches, out = timed(store, tile, False, args.steps, args.warmup, depth)
     total_bf16 = max_over_ranks(total_bf16, world)
     fwd_b, bwd_b, counts = compositor_bytes(out[-1], 3, R, 2, N, C, H, W)
     del out  # no live autograd graph may reach the leaves when a CUDA graph is captured
     graphed = None
     if not args.no_graph:
-        graphed = time_graphed(lambda: step(store, tile, False), args.steps, C * H * W * world)
+        graphed = time_graphed(lambda: step(store, tile, False, depth), args.steps, C * H * W * world)
     # FP32 plain drop-in on the same GPU: FP32 textures, one camera per call, tile 16
     total_f32, per_f32, stages_f32, launches_f32, _ = timed(None, 16, True, args.steps, args.warmup)
     total_f32 = max_over_ranks(total_f32, world)
@@ -314,8 +317,9 @@ def _run_ours(args, rank, world, local, dev):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, shapes of the workload)",
         "config": {"workload": f"mixture1m: N={N:,} splats, {R}x{R} RGBA textures sampled from BF16 storage "
                                f"(FP32 master + FP32 gradients), {C} cameras 1600x1200 per GPU in one call, "
-                               f"tile {tile} (autotuned), fwd+bwd",
-                   "texture_storage": "bf16", "tile_size": tile, "tile_tuning_ms": tune_ms, "splats": N,
+                               f"tile {tile}, batch depth {depth or tile * tile} (autotuned), fwd+bwd",
+                   "texture_storage": "bf16", "tile_size": tile, "batch_depth": depth or tile * tile,
+                   "tuning_ms": tune_ms, "splats": N,
                    "tile_order": args.tile_order,
                    "cameras_per_gpu": C, "width": W, "height": H,
                    "l2": "inputs larger than L2 (BF16 textures 8.4 GB, FP32 master 16.8 GB)",
@@ -521,7 +525,7 @@ def _run_batch(args, dev):
     from textured_gaussians_b200 import rasterization_textured_gaussians
     from textured_gaussians_b200.batch import ViewTable, rasterization_textured_gaussians_batch
     from textured_gaussians_b200.cuda import make_texture_storage
-    from textured_gaussians_b200.tuning import autotune_tile_size
+    from textured_gaussians_b200.tuning import autotune_compositor
 
     cat, offs, V, K, sizes, vs = make_batch_workload(n_views=args.views)
     T = lambda x: torch.from_numpy(x).to(dev)
@@ -544,7 +548,7 @@ def _run_batch(args, dev):
         for t in list(L.values()) + [tex32]:
             t.grad = None
 
-    def step_batch(tile, order):
+    def step_batch(tile, order, depth=0):
         zero()
         vt = tables.get(tile)
         if vt is None:
@@ -552,7 +556,7 @@ def _run_batch(args, dev):
         out = rasterization_textured_gaussians_batch(
             L["means"], L["quats"], L["scales"], L["opacities"], L["colors"], tex32, offs, viewmats, Ks, widths,
             heights, vs, sh_degree=0, far_plane=100.0, tile_size=tile, texture_storage=store, tile_order=order,
-            view_table=vt)
+            view_table=vt, batch_depth=depth)
         meta = out[-1]
         loss = (meta["flat_colors"] * w_flat[:, :3]).sum() + (meta["flat_alphas"] * w_flat[:, 3:]).sum()
         loss.backward()
@@ -586,12 +590,13 @@ def _run_batch(args, dev):
         B.TIMERS.enable(False)
         return t0.elapsed_time(t1) / steps, stages, B.lib().tg_kernel_launch_count() - l0
 
-    tile, tune_ms = autotune_tile_size(("batch", N, len(sizes)), lambda ts: step_batch(ts, "heaviest_first"),
-                                       repeats=1)
+    (tile, depth), tune_ms = autotune_compositor(("batch", N, len(sizes)),
+                                                 lambda ts, d: step_batch(ts, "heaviest_first", d), repeats=1)
     with ClockSampler(0) as clk:
-        ms_b, stages_b, launches_b = timed(lambda: step_batch(tile, "heaviest_first"), args.steps, args.warmup)
-    ms_launch, _, _ = timed(lambda: step_batch(tile, "launch"), args.steps, 1)
-    graphed = None if args.no_graph else time_graphed(lambda: step_batch(tile, "heaviest_first"), args.steps, n_pix)
+        ms_b, stages_b, launches_b = timed(lambda: step_batch(tile, "heaviest_first", depth), args.steps, args.warmup)
+    ms_launch, _, _ = timed(lambda: step_batch(tile, "launch", depth), args.steps, 1)
+    graphed = (None if args.no_graph
+               else time_graphed(lambda: step_batch(tile, "heaviest_first", depth), args.steps, n_pix))
     ms_pv, stages_pv, launches_pv = timed(step_per_view, args.steps, 1)
     line = {
         "metric": "textured 2DGS fwd+bwd Mpix/s, batching form: 64 uneven views over 3 scenes in one call",
@@ -600,8 +605,9 @@ def _run_batch(args, dev):
         "data": "synthetic (seeded)",
         "config": {"workload": f"3 mixture scenes N=200k/500k/1M ({N:,} splats), {R}x{R} RGBA textures in BF16 "
                                f"storage, {len(sizes)} views drawn from {BATCH_SIZES}, {n_pix:,} pixels, "
-                               f"tile {tile} (autotuned), heaviest tiles first, fwd+bwd",
-                   "tile_tuning_ms": tune_ms, "views": len(sizes), "pixels": n_pix, "splats": N},
+                               f"tile {tile}, batch depth {depth or tile * tile} (autotuned), heaviest tiles first, "
+                               f"fwd+bwd",
+                   "tuning_ms": tune_ms, "views": len(sizes), "pixels": n_pix, "splats": N},
         "splats_per_s": round(sum(offs[s + 1] - offs[s] for s in vs) / (ms_b / 1e3), 1),
         "launch_order_ms_per_step": round(ms_launch, 3),
         "per_view_fp32": {"value": round(n_pix / (ms_pv / 1e3) / 1e6, 2), "unit": "Mpix/s",
@@ -647,7 +653,9 @@ def main():
     ap.add_argument("--cameras", type=int, default=4)
     ap.add_argument("--tex", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=16)
-    ap.add_argument("--tile", type=int, default=0, help="tile size of the headline form (0 = autotune over 8, 16)")
+    ap.add_argument("--tile", type=int, default=0,
+                    help="tile size of the headline form (0 = autotune tile over 8, 16, 32 and the batch depth)")
+    ap.add_argument("--depth", type=int, default=0, help="batch depth with --tile (0 = tile^2)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay timing")

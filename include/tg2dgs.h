@@ -30,7 +30,7 @@ typedef struct CUstream_st* tg_stream_t; /* same type as cudaStream_t */
 
 #define TG_OK 0
 #define TG_ERR_INVALID_ARG (-1)   /* null pointer, bad size, misaligned buffer */
-#define TG_ERR_UNSUPPORTED (-2)   /* channel count / texture format / tile size not supported */
+#define TG_ERR_UNSUPPORTED (-2)   /* channel count / texture format / tile size (8, 16, 32) not supported */
 #define TG_ERR_CUDA (-3)          /* a CUDA launch or runtime call failed */
 #define TG_ERR_WORKSPACE (-4)     /* workspace smaller than tg_sort_workspace_bytes() */
 #define TG_ERR_TIMEOUT (-5)       /* a bounded device-side wait gave up */
@@ -337,6 +337,9 @@ typedef struct {
     /* Capacity mode: device count of valid intersections (flatten_ids then
      * holds n_isects >= *n_isects_dev entries, the tail unused), or NULL. */
     const int64_t* n_isects_dev;
+    /* Splats staged in shared memory per batch: 0 = tile_size^2 (the
+     * reference's batch), else a multiple of 32 up to 1024. */
+    int32_t batch_depth;
 } tg_raster_fwd_args;
 TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
 

@@ -223,7 +223,7 @@ def test_plain_forward(name):
     _compare_fwd(g, o, 1e-4)
 
 
-def _grads_gpu(s, d, textured, filtering, bg=None, absgrad=False, seed=3):
+def _grads_gpu(s, d, textured, filtering, bg=None, absgrad=False, seed=3, depth=0):
     rng = np.random.default_rng(seed)
     C, H, W = d["C"], s.height, s.width
     up = dict(c=rng.normal(size=(C, H, W, 3)), a=rng.normal(size=(C, H, W, 1)), n=rng.normal(size=(C, H, W, 3)),
@@ -239,10 +239,10 @@ def _grads_gpu(s, d, textured, filtering, bg=None, absgrad=False, seed=3):
     if textured:
         out = rasterize_to_pixels_textured_gaussians(
             m2d, M, cols, opac, tex, 3.0, 3.0, nrm, dens, W, H, s.tile_size, d["off"], d["fl"],
-            backgrounds=None if bg is None else T(bg), absgrad=absgrad, filtering=filtering)
+            backgrounds=None if bg is None else T(bg), absgrad=absgrad, filtering=filtering, batch_depth=depth)
     else:
         out = rasterize_to_pixels_2dgs(m2d, M, cols, opac, nrm, dens, W, H, s.tile_size, d["off"], d["fl"],
-                                       backgrounds=None if bg is None else T(bg), absgrad=absgrad)
+                                       backgrounds=None if bg is None else T(bg), absgrad=absgrad, batch_depth=depth)
     loss = ((out[0] * T(up["c"])).sum() + (out[1] * T(up["a"])).sum() + (out[2] * T(up["n"])).sum()
             + (out[3] * T(up["d"])).sum() + (out[4] * T(up["m"])).sum())
     loss.backward()
@@ -358,3 +358,37 @@ def test_sort_bounded_wait_gives_up_with_a_status_and_the_context_survives():
     k2, v2 = sort_pairs(keys.clone(), vals.clone(), 40, check=True)
     ref = torch.sort(keys, stable=True)
     assert torch.equal(k2, ref.values) and torch.equal(v2.long(), ref.indices)
+
+
+@pytest.mark.parametrize("tile,textured", [(32, True), (32, False), (8, True)])
+def test_other_tile_sizes_match_oracle(tile, textured):
+    """32x32 tiles (four pixels per thread) and 8x8 tiles against the FP64 oracle run with the same tile size."""
+    s = scenes.small()
+    s.tile_size = tile
+    d = _raster_inputs(s)
+    g, up, out = _grads_gpu(s, d, textured, "bilinear_exact" if textured else None)
+    fo = _oracle_fwd(s, d, textured)
+    _compare_fwd(out, fo, 1e-4)
+    o = O.raster_bwd(to_np(d["means2d"]), to_np(d["M"]), d["colors"], d["opac"], to_np(d["normals"]),
+                     d["deq"] if textured else None, d["off"].cpu().numpy(), d["fl"].cpu().numpy(), s.width,
+                     s.height, tile, fo, up["c"], up["a"], up["n"], up["d"], up["m"], mode=2 if textured else 0,
+                     dtype=F64)
+    pairs = [("means2d", o.v_means2d), ("M", o.v_M), ("colors", o.v_colors), ("opac", o.v_opacities),
+             ("normals", o.v_normals)] + ([("textures", o.v_textures)] if textured else [])
+    for k, ref in pairs:
+        assert rel_l2(to_np(g[k]), ref) < 1e-4, (k, rel_l2(to_np(g[k]), ref))
+
+
+@pytest.mark.parametrize("tile,depth", [(8, 32), (8, 256), (16, 64), (16, 1024), (32, 256)])
+def test_batch_depth_changes_nothing(tile, depth):
+    """The staging depth only regroups the same front-to-back / back-to-front sweep:
+    forward outputs bit-exact, gradients equal up to float-atomic order."""
+    s = scenes.small()
+    s.tile_size = tile
+    d = _raster_inputs(s)
+    g0, _, out0 = _grads_gpu(s, d, True, "bilinear_exact")
+    g1, _, out1 = _grads_gpu(s, d, True, "bilinear_exact", depth=depth)
+    for a, b in zip(out0[:5], out1[:5]):  # per-pixel outputs (the statistics are float atomics)
+        assert torch.equal(a, b)
+    for k in ("means2d", "M", "colors", "opac", "normals", "textures", "densify"):
+        assert rel_l2(to_np(g1[k]), to_np(g0[k])) < 1e-6, k

@@ -69,7 +69,8 @@ class RasterFwdArgs(ctypes.Structure):
                 ("gaussian_ids", P), ("contrib_threshold", F32), ("g_weight", F32), ("n_contrib", I32),
                 ("out_colors", P), ("out_alphas", P), ("out_normals", P), ("out_distort", P), ("out_median", P),
                 ("last_ids", P), ("median_ids", P), ("contrib_sum", P), ("contrib_count", P), ("tile_order", P),
-                ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64), ("n_isects_dev", P)]
+                ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64), ("n_isects_dev", P),
+                ("batch_depth", I32)]
 
 
 class RasterBwdArgs(ctypes.Structure):

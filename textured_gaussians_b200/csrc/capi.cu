@@ -91,8 +91,10 @@ int64_t raster_pixels(const tg_raster_fwd_args& a) {
 
 int check_raster_common(const tg_raster_fwd_args& a) {
     TG_REQUIRE(a.C >= 0 && a.width >= 0 && a.height >= 0, TG_ERR_INVALID_ARG, "negative sizes");
-    TG_REQUIRE(a.tile_size == 16 || a.tile_size == 8, TG_ERR_UNSUPPORTED, "tile_size %d not supported (8 or 16)",
-               a.tile_size);
+    TG_REQUIRE(a.tile_size == 8 || a.tile_size == 16 || a.tile_size == 32, TG_ERR_UNSUPPORTED,
+               "tile_size %d not supported (8, 16 or 32)", a.tile_size);
+    TG_REQUIRE(a.batch_depth == 0 || (a.batch_depth >= 32 && a.batch_depth <= 1024 && a.batch_depth % 32 == 0),
+               TG_ERR_UNSUPPORTED, "batch_depth %d not supported (0, or a multiple of 32 up to 1024)", a.batch_depth);
     TG_REQUIRE(a.D >= 1 && a.D <= 5, TG_ERR_UNSUPPORTED, "unsupported number of channels: %d", a.D);
     if (a.views) {
         TG_REQUIRE(a.tile_view && a.n_tiles >= 0 && a.n_tiles < (int64_t(1) << 31) && a.n_pixels >= 0,

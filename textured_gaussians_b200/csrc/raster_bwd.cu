@@ -1,6 +1,7 @@
 // Textured / plain 2DGS compositor, adjoint, for sm_100a.
 //
-// One CTA per (camera, tile), one thread per pixel, back-to-front over the
+// One CTA per (camera, tile) work item, one thread per pixel (four for 32x32
+// tiles), back-to-front in batches of `batch_depth` staged splats over the
 // splats that can still matter to the tile (batches beyond every pixel's last
 // contributor are skipped).  Transmittance is recovered from the stored final
 // T and last-contributor index by division, as the reference does
@@ -57,10 +58,12 @@ struct GradSlots {
 #ifndef TG_BWD_MIN_CTAS
 #define TG_BWD_MIN_CTAS 2
 #endif
-// Pixels per thread for 16x16 tiles.
-#ifndef TG_BWD_PPT
-#define TG_BWD_PPT 1
-#endif
+// Register budget: TG_BWD_MIN_CTAS resident CTAs for one pixel per thread,
+// one CTA of 256 threads for the four-pixel (32x32 tile) form.
+template <int PPT>
+struct BwdBounds {
+    static constexpr int kMinCtas = PPT == 1 ? TG_BWD_MIN_CTAS : 1;
+};
 
 // Per-pixel state of the back-to-front sweep.
 template <int D>
@@ -196,14 +199,14 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
 }
 
 template <int D, class Tex, int PPT>
-__global__ void __launch_bounds__(256 / PPT, TG_BWD_MIN_CTAS) raster_bwd_kernel(const tg_raster_bwd_args a,
-                                                                                const float uv_scale) {
+__global__ void __launch_bounds__(256, BwdBounds<PPT>::kMinCtas) raster_bwd_kernel(const tg_raster_bwd_args a,
+                                                                                   const float uv_scale,
+                                                                                   const int bs) {
     using GS = GradSlots<D>;
     constexpr int NV = GS::kCount;
     const tg_raster_fwd_args& f = a.f;
     extern __shared__ float4 smem4[];
-    const int nt = blockDim.x;
-    const int bs = nt * PPT;  // splats per batch = tile_size^2
+    const int nt = blockDim.x;  // tile_size^2 / PPT threads; bs = splats staged per batch
     float4* s_box = smem4;  // per-splat cull box (see cull_box)
     float4* s_xyo = s_box + bs;
     float4* s_m0 = s_xyo + bs;
@@ -299,9 +302,7 @@ __global__ void __launch_bounds__(256 / PPT, TG_BWD_MIN_CTAS) raster_bwd_kernel(
         if (batch_end - (bs - 1) > block_max_bin) continue;  // every splat here is past all last contributors
         const int32_t batch_size = min(bs, batch_end + 1 - range_start);
         __syncthreads();  // previous batch fully flushed before restaging
-#pragma unroll
-        for (int q = 0; q < PPT; ++q) {
-            const int slot = tr + q * nt;
+        for (int slot = tr; slot < bs; slot += nt) {
             const int32_t idx_load = batch_end - slot;
             if (idx_load >= range_start) {
                 const int32_t g = f.flatten_ids[idx_load];
@@ -382,25 +383,29 @@ __global__ void densify_grad_kernel(const float* __restrict__ v_M, const float* 
     v_densify[2 * e + 1] = v_M[9 * e + 5] * depth;
 }
 
+size_t bwd_smem_bytes(int D, int bs) {
+    return (size_t)bs * (6 * sizeof(float4) + D * sizeof(float) + 2 * sizeof(int) + (D + 17) * sizeof(float));
+}
+
 template <int D, class Tex>
 cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     const tg_raster_fwd_args& f = a.f;
     const int tile_px = f.tile_size * f.tile_size;
-    const size_t smem = (size_t)tile_px * (6 * sizeof(float4) + D * sizeof(float) + 2 * sizeof(int) +
-                                           GradSlots<D>::kCount * sizeof(float));
+    const int bs = f.batch_depth > 0 ? f.batch_depth : tile_px;
+    const size_t smem = bwd_smem_bytes(D, bs);
     const int64_t blocks = f.views ? f.n_tiles : (int64_t)f.C * f.tile_width * f.tile_height;
     const float uv_scale = a.adjoint == TG_ADJ_BWD2 ? 1.f : (a.adjoint == TG_ADJ_EXACT ? 0.5f : 0.f);
-    const bool multi = tile_px >= 64 * TG_BWD_PPT;
-    cudaError_t err = multi ? cudaFuncSetAttribute(raster_bwd_kernel<D, Tex, TG_BWD_PPT>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                            : cudaFuncSetAttribute(raster_bwd_kernel<D, Tex, 1>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const bool four = tile_px > 256;  // 32x32 tiles: four pixels per thread, 256 threads
+    cudaError_t err = four ? cudaFuncSetAttribute(raster_bwd_kernel<D, Tex, 4>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                           : cudaFuncSetAttribute(raster_bwd_kernel<D, Tex, 1>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     if (blocks > 0 && f.n_isects > 0) {
-        if (multi)
-            raster_bwd_kernel<D, Tex, TG_BWD_PPT><<<(unsigned)blocks, tile_px / TG_BWD_PPT, smem, s>>>(a, uv_scale);
+        if (four)
+            raster_bwd_kernel<D, Tex, 4><<<(unsigned)blocks, tile_px / 4, smem, s>>>(a, uv_scale, bs);
         else
-            raster_bwd_kernel<D, Tex, 1><<<(unsigned)blocks, tile_px, smem, s>>>(a, uv_scale);
+            raster_bwd_kernel<D, Tex, 1><<<(unsigned)blocks, tile_px, smem, s>>>(a, uv_scale, bs);
         note_launches(1);
     }
     if ((err = cudaGetLastError()) != cudaSuccess) return err;

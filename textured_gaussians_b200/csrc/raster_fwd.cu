@@ -1,11 +1,12 @@
 // Textured / plain 2DGS compositor, forward, for sm_100a.
 //
 // One CTA per (camera, tile) work item, front-to-back over the tile's depth-sorted
-// splats in batches of tile_size^2 splats staged in shared memory (the gather
-// of each splat's record happens once per CTA, not once per pixel).  Each
-// thread owns PPT pixels of the tile (rows r and r + tile/PPT): the PPT
-// evaluations of a splat are independent, so their texture loads are in flight
-// together, and the splat's shared-memory record is read once for all of them.
+// splats in batches of `batch_depth` splats (tile_size^2 by default) staged in
+// shared memory (the gather of each splat's record happens once per CTA, not
+// once per pixel).  8x8 and 16x16 tiles run one thread per pixel; 32x32 tiles
+// run 256 threads owning PPT = 4 pixels each (rows r, r+8, r+16, r+24): the
+// PPT evaluations of a splat are independent, so their texture loads are in
+// flight together, and the splat's shared-memory record is read once for all.
 // Each pixel samples its splat's RGBA texture with one 16-byte (FP32), 8-byte
 // (BF16/FP16) or 4-byte (FP8) load per bilinear tap and reuses the four taps for
 // the alpha scale and every colour channel.  A warp whose pixels are all
@@ -25,17 +26,20 @@ namespace tg {
 #ifndef TG_FWD_MIN_CTAS
 #define TG_FWD_MIN_CTAS 4
 #endif
-// Pixels per thread for 16x16 tiles.
-#ifndef TG_FWD_PPT
-#define TG_FWD_PPT 1
-#endif
+
+// Register budget: 4 resident CTAs of 256 threads for one pixel per thread;
+// one CTA for the four-pixel (32x32 tile) form.
+template <int PPT>
+struct FwdBounds {
+    static constexpr int kMinCtas = PPT == 1 ? TG_FWD_MIN_CTAS : 1;
+};
 
 template <int D, class Tex, int PPT>
-__global__ void __launch_bounds__(256 / PPT, TG_FWD_MIN_CTAS) raster_fwd_kernel(const tg_raster_fwd_args a) {
+__global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kernel(const tg_raster_fwd_args a,
+                                                                                   const int bs) {
     constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
     extern __shared__ float4 smem4[];
-    const int nt = blockDim.x;  // threads; the batch holds nt * PPT = tile_size^2 splats
-    const int bs = nt * PPT;
+    const int nt = blockDim.x;  // threads: tile_size^2 / PPT; bs = splats staged per batch
     float4* s_box = smem4;  // per-splat cull box (see cull_box)
     float4* s_xyo = s_box + bs;
     float4* s_m0 = s_xyo + bs;
@@ -119,9 +123,7 @@ __global__ void __launch_bounds__(256 / PPT, TG_FWD_MIN_CTAS) raster_fwd_kernel(
         for (int q = 0; q < PPT; ++q) all_done &= done[q];
         if (__syncthreads_count(all_done) >= nt) break;
         const int32_t batch_start = range_start + bs * b;
-#pragma unroll
-        for (int q = 0; q < PPT; ++q) {
-            const int slot = tr + q * nt;
+        for (int slot = tr; slot < bs; slot += nt) {
             const int32_t idx = batch_start + slot;
             if (idx < range_end) {
                 const int32_t g = a.flatten_ids[idx];
@@ -219,16 +221,26 @@ __global__ void __launch_bounds__(256 / PPT, TG_FWD_MIN_CTAS) raster_fwd_kernel(
     }
 }
 
+size_t fwd_smem_bytes(int D, int bs) { return (size_t)bs * (6 * sizeof(float4) + D * sizeof(float) + sizeof(int)); }
+
 template <int D, class Tex>
 cudaError_t launch_fwd_t(const tg_raster_fwd_args& a, cudaStream_t s) {
     const int tile_px = a.tile_size * a.tile_size;
-    const size_t smem = (size_t)tile_px * (6 * sizeof(float4) + D * sizeof(float) + sizeof(int));
+    const int bs = a.batch_depth > 0 ? a.batch_depth : tile_px;
+    const size_t smem = fwd_smem_bytes(D, bs);
     const int64_t blocks = a.views ? a.n_tiles : (int64_t)a.C * a.tile_width * a.tile_height;
     if (blocks == 0) return cudaSuccess;
-    if (tile_px >= 64 * TG_FWD_PPT) {
-        raster_fwd_kernel<D, Tex, TG_FWD_PPT><<<(unsigned)blocks, tile_px / TG_FWD_PPT, smem, s>>>(a);
+    cudaError_t err;
+    if (tile_px > 256) {  // 32x32 tiles: four pixels per thread, 256 threads
+        err = cudaFuncSetAttribute(raster_fwd_kernel<D, Tex, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem);
+        if (err != cudaSuccess) return err;
+        raster_fwd_kernel<D, Tex, 4><<<(unsigned)blocks, tile_px / 4, smem, s>>>(a, bs);
     } else {
-        raster_fwd_kernel<D, Tex, 1><<<(unsigned)blocks, tile_px, smem, s>>>(a);
+        err = cudaFuncSetAttribute(raster_fwd_kernel<D, Tex, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem);
+        if (err != cudaSuccess) return err;
+        raster_fwd_kernel<D, Tex, 1><<<(unsigned)blocks, tile_px, smem, s>>>(a, bs);
     }
     note_launches(1);
     return cudaGetLastError();

@@ -539,7 +539,8 @@ def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_stor
         int(n_contrib), None, None, None, None, None, None, None, None, None,
         None if layout is None else B.ptr(layout.get("tile_order")),
         None if vt is None else B.ptr(vt.views), None if vt is None else B.ptr(vt.tile_view),
-        0 if vt is None else vt.n_tiles, 0 if vt is None else vt.n_pixels, B.ptr(n_isects_dev))
+        0 if vt is None else vt.n_tiles, 0 if vt is None else vt.n_pixels, B.ptr(n_isects_dev),
+        0 if layout is None else layout.get("batch_depth", 0))
 
 
 class _RasterizeToPixelsTextured(torch.autograd.Function):
@@ -648,12 +649,12 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
                 None)
 
 
-def _layout(tile_order, view_table):
-    if tile_order is None and view_table is None:
+def _layout(tile_order, view_table, batch_depth=0):
+    if tile_order is None and view_table is None and not batch_depth:
         return None
     if tile_order is not None:
         tile_order = tile_order.to(torch.int32).contiguous()
-    return {"tile_order": tile_order, "view_table": view_table}
+    return {"tile_order": tile_order, "view_table": view_table, "batch_depth": int(batch_depth or 0)}
 
 
 def _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
@@ -712,6 +713,7 @@ def rasterize_to_pixels_textured_gaussians(
     gaussian_ids: Optional[Tensor] = None,
     tile_order: Optional[Tensor] = None,
     view_table=None,
+    batch_depth: int = 0,
 ) -> Tuple[Tensor, ...]:
     """Rasterize textured 2D Gaussians to pixels (reference: cuda/_wrapper.py:1806-2002).
 
@@ -731,7 +733,8 @@ def rasterize_to_pixels_textured_gaussians(
     :func:`tile_order_heaviest_first`) sets the order in which tiles are
     taken; ``view_table`` selects the batching form (views of uneven size,
     flat ``isect_offsets`` from :func:`isect_offset_encode_views`, flat
-    per-pixel outputs [n_pixels, ...]).
+    per-pixel outputs [n_pixels, ...]).  ``batch_depth`` sets how many splats
+    are staged in shared memory per batch (0: tile_size^2, the reference's).
     """
     _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
                   backgrounds, packed, view_table)
@@ -759,7 +762,8 @@ def rasterize_to_pixels_textured_gaussians(
         None if backgrounds is None else backgrounds.contiguous(), masks, store, texture_scales,
         float(texture_range_x), float(texture_range_y), int(image_width), int(image_height), int(tile_size),
         isect_offsets.contiguous(), flatten_ids.contiguous(), absgrad, gs_contrib_threshold, g_weight,
-        _FILTER_ADJOINT[filtering], False, gaussian_ids, textures.shape[0], _layout(tile_order, view_table))
+        _FILTER_ADJOINT[filtering], False, gaussian_ids, textures.shape[0],
+        _layout(tile_order, view_table, batch_depth))
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]
@@ -789,6 +793,7 @@ def rasterize_to_pixels_2dgs(
     n_gaussians: Optional[int] = None,
     tile_order: Optional[Tensor] = None,
     view_table=None,
+    batch_depth: int = 0,
 ) -> Tuple[Tensor, ...]:
     """Rasterize plain 2D Gaussians to pixels (reference: cuda/_wrapper.py:1647-1784).
 
@@ -796,8 +801,9 @@ def rasterize_to_pixels_2dgs(
     when the backgrounds require it (reference: cuda/_wrapper.py:2920-2925).
     Packed inputs: the contribution statistics are per entry, [nnz], or per
     Gaussian, [n_gaussians], when ``gaussian_ids`` and ``n_gaussians`` are
-    given (the reference sizes them [0] for packed inputs).  ``tile_order`` and
-    ``view_table`` as in :func:`rasterize_to_pixels_textured_gaussians`.
+    given (the reference sizes them [0] for packed inputs).  ``tile_order``,
+    ``view_table`` and ``batch_depth`` as in
+    :func:`rasterize_to_pixels_textured_gaussians`.
     """
     _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
                   backgrounds, packed, view_table)
@@ -815,7 +821,7 @@ def rasterize_to_pixels_2dgs(
         normals.contiguous(), densify.contiguous(), None if backgrounds is None else backgrounds.contiguous(), masks,
         None, None, 3.0, 3.0, int(image_width), int(image_height), int(tile_size), isect_offsets.contiguous(),
         flatten_ids.contiguous(), absgrad, gs_contrib_threshold, 1.0, B.TG_ADJ_REFERENCE, True, gaussian_ids,
-        int(n_gaussians), _layout(tile_order, view_table))
+        int(n_gaussians), _layout(tile_order, view_table, batch_depth))
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]

@@ -17,7 +17,9 @@ Extensions (keyword-only, default off): ``texture_storage`` /
 ``textures``), ``filtering="bilinear_exact"`` and ``adjoint="exact"`` (exact
 adjoint end to end), ``tile_order`` ("heaviest_first", the default: compositor
 tiles taken by descending intersection count, so the longest tiles do not form
-the launch's tail; "launch": tile index order; the results are the same).
+the launch's tail; "launch": tile index order; the results are the same),
+``batch_depth`` (splats staged per compositor batch; 0 = tile_size^2) and
+``tile_size`` 32 besides the reference's 8 and 16.
 """
 from __future__ import annotations
 
@@ -182,6 +184,7 @@ def rasterization_2dgs(
     *,
     adjoint: str = "reference",
     tile_order: str = "heaviest_first",
+    batch_depth: int = 0,
 ) -> Tuple[Tensor, Tensor, Tensor, Optional[Tensor], Tensor, Tensor, Tensor, Tensor, Dict]:
     """Rasterize 2D Gaussian surfels (N) to C image planes (reference: rendering.py:1009-1338).
 
@@ -196,7 +199,7 @@ def rasterization_2dgs(
         p["means2d"], p["ray_transforms"], p["colors"], p["opacities"], p["normals"], p["densify"], width, height,
         tile_size, p["isect_offsets"], p["flatten_ids"], backgrounds=backgrounds, packed=packed, absgrad=absgrad,
         distloss=distloss, gs_contrib_threshold=gs_contrib_threshold, gaussian_ids=p["gaussian_ids"],
-        n_gaussians=means.shape[0] if packed else None, tile_order=p["tile_order"])
+        n_gaussians=means.shape[0] if packed else None, tile_order=p["tile_order"], batch_depth=batch_depth)
     return _finish(p, *outs, viewmats, Ks, width, height, tile_size, render_mode, depth_mode)
 
 
@@ -235,6 +238,7 @@ def rasterization_textured_gaussians(
     texture_scales: Optional[Tensor] = None,
     adjoint: str = "reference",
     tile_order: str = "heaviest_first",
+    batch_depth: int = 0,
 ) -> Tuple[Tensor, Tensor, Tensor, Optional[Tensor], Tensor, Tensor, Tensor, Tensor, Dict]:
     """Rasterize textured 2D Gaussian surfels (reference: rendering.py:1342-1685).
 
@@ -253,5 +257,5 @@ def rasterization_textured_gaussians(
         backgrounds=backgrounds, packed=packed, absgrad=absgrad, distloss=distloss,
         gs_contrib_threshold=gs_contrib_threshold, filtering=filtering, g_weight=g_weight,
         texture_storage=texture_storage, texture_scales=texture_scales, gaussian_ids=p["gaussian_ids"],
-        tile_order=p["tile_order"])
+        tile_order=p["tile_order"], batch_depth=batch_depth)
     return _finish(p, *outs, viewmats, Ks, width, height, tile_size, render_mode, depth_mode)
