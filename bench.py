@@ -104,6 +104,7 @@ class ClockSampler:
         self.index = index
         self.rows = []
         self.proc = None
+        self.marked = False
 
     def __enter__(self):
         try:
@@ -118,7 +119,12 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            if self.marked:  # only samples taken from the timed region on
+                self.rows.append([x.strip() for x in line.split(",")])
+
+    def mark(self):
+        """Start keeping samples (the timed region begins)."""
+        self.marked = True
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -225,7 +231,7 @@ def _run_ours(args, rank, world, local, dev):
     w_rgb = torch.randn((C, H, W, 3), generator=g, device=dev)
     w_a = torch.randn((C, H, W, 1), generator=g, device=dev)
 
-    def step(storage, tile_size, per_view, depth=0):
+    def step(storage, tile_size, per_view, depth=0, persistent=False):
         for t in (means, quats, scales, opac, colors, tex32):
             t.grad = None
         views = [slice(c, c + 1) for c in range(C)] if per_view else [slice(0, C)]
@@ -233,7 +239,8 @@ def _run_ours(args, rank, world, local, dev):
             out = rasterization_textured_gaussians(means, quats, scales, opac, colors, tex32, viewmats[v], Ks[v], W, H,
                                                    sh_degree=0, far_plane=100.0, tile_size=tile_size,
                                                    texture_storage=storage,
-                                                   tile_order=args.tile_order, batch_depth=depth)
+                                                   tile_order=args.tile_order, batch_depth=depth,
+                                                   persistent=persistent)
             loss = (out[0] * w_rgb[v]).sum() + (out[1] * w_a[v]).sum()
             loss.backward()
         return out, loss
@@ -269,18 +276,22 @@ def _run_ours(args, rank, world, local, dev):
     # batch depth autotuned
     from textured_gaussians_b200.tuning import autotune_compositor
 
-    if args.tile:
-        (tile, depth), tune_ms = (args.tile, args.depth), {}
-    else:
-        (tile, depth), tune_ms = autotune_compositor(("bench", N, C, W, H, R),
-                                                     lambda ts, d: step(store, ts, False, d))
-        tile = int(max_over_ranks(float(tile), world))  # every rank uses the same configuration
-        depth = int(max_over_ranks(float(depth), world))
+    # the clock sampler starts before tuning and warm-up, so its own start-up never overlaps the timed steps
     with ClockSampler(local) as clk:
+        if args.tile:
+            (tile, depth), tune_ms = (args.tile, args.depth), {}
+        else:
+            (tile, depth), tune_ms = autotune_compositor(("bench", N, C, W, H, R),
+                                                         lambda ts, d: step(store, ts, False, d))
+            tile = int(max_over_ranks(float(tile), world))  # every rank uses the same configuration
+            depth = int(max_over_ranks(float(depth), world))
+        clk.mark()
         total_bf16, per_bf16, stages_bf16, launches, out = timed(store, tile, False, args.steps, args.warmup, depth)
     total_bf16 = max_over_ranks(total_bf16, world)
     fwd_b, bwd_b, counts = compositor_bytes(out[-1], 3, R, 2, N, C, H, W)
     del out  # no live autograd graph may reach the leaves when a CUDA graph is captured
+    # the same form with the persistent compositor launch (CTAs take tiles from a work counter)
+    pers_ms = timed_plain(lambda: step(store, tile, False, depth, True), args.steps)
     graphed = None
     if not args.no_graph:
         graphed = time_graphed(lambda: step(store, tile, False, depth), args.steps, C * H * W * world)
@@ -330,11 +341,28 @@ def _run_ours(args, rank, world, local, dev):
                        "stage_ms": stage_ms_f32},
         "bf16_over_fp32": round(value / value_f32, 3),
         "stage_ms": stage_ms, "per_step_ms": [round(x, 3) for x in per_bf16],
-        "graphed": graphed,
+        "graphed": graphed, "persistent_ms_per_step": round(pers_ms, 3),
         "counts": counts, "roofline": roofline, "gpu_launches": int(launches),
         "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
+
+
+def timed_plain(fn, steps, warmup=1):
+    """Mean CUDA-event ms per call of fn() after `warmup` calls (current stream)."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        fn()
+    t1.record()
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) / steps
 
 
 def time_graphed(fn, steps, pixels):
@@ -548,7 +576,7 @@ def _run_batch(args, dev):
         for t in list(L.values()) + [tex32]:
             t.grad = None
 
-    def step_batch(tile, order, depth=0):
+    def step_batch(tile, order, depth=0, persistent=False):
         zero()
         vt = tables.get(tile)
         if vt is None:
@@ -556,7 +584,7 @@ def _run_batch(args, dev):
         out = rasterization_textured_gaussians_batch(
             L["means"], L["quats"], L["scales"], L["opacities"], L["colors"], tex32, offs, viewmats, Ks, widths,
             heights, vs, sh_degree=0, far_plane=100.0, tile_size=tile, texture_storage=store, tile_order=order,
-            view_table=vt, batch_depth=depth)
+            view_table=vt, batch_depth=depth, persistent=persistent)
         meta = out[-1]
         loss = (meta["flat_colors"] * w_flat[:, :3]).sum() + (meta["flat_alphas"] * w_flat[:, 3:]).sum()
         loss.backward()
@@ -593,8 +621,10 @@ def _run_batch(args, dev):
     (tile, depth), tune_ms = autotune_compositor(("batch", N, len(sizes)),
                                                  lambda ts, d: step_batch(ts, "heaviest_first", d), repeats=1)
     with ClockSampler(0) as clk:
+        clk.mark()
         ms_b, stages_b, launches_b = timed(lambda: step_batch(tile, "heaviest_first", depth), args.steps, args.warmup)
     ms_launch, _, _ = timed(lambda: step_batch(tile, "launch", depth), args.steps, 1)
+    ms_pers = timed_plain(lambda: step_batch(tile, "heaviest_first", depth, True), args.steps)
     graphed = (None if args.no_graph
                else time_graphed(lambda: step_batch(tile, "heaviest_first", depth), args.steps, n_pix))
     ms_pv, stages_pv, launches_pv = timed(step_per_view, args.steps, 1)
@@ -609,7 +639,7 @@ def _run_batch(args, dev):
                                f"fwd+bwd",
                    "tuning_ms": tune_ms, "views": len(sizes), "pixels": n_pix, "splats": N},
         "splats_per_s": round(sum(offs[s + 1] - offs[s] for s in vs) / (ms_b / 1e3), 1),
-        "launch_order_ms_per_step": round(ms_launch, 3),
+        "launch_order_ms_per_step": round(ms_launch, 3), "persistent_ms_per_step": round(ms_pers, 3),
         "per_view_fp32": {"value": round(n_pix / (ms_pv / 1e3) / 1e6, 2), "unit": "Mpix/s",
                           "ms_per_step": round(ms_pv, 3), "form": "FP32 plain drop-in, one call per view, tile 16",
                           "stage_ms": stages_pv, "gpu_launches": int(launches_pv)},

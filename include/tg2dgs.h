@@ -340,6 +340,10 @@ typedef struct {
     /* Splats staged in shared memory per batch: 0 = tile_size^2 (the
      * reference's batch), else a multiple of 32 up to 1024. */
     int32_t batch_depth;
+    /* Persistent launch: one device uint32 the call zeroes; a grid of as many
+     * CTAs as fit on the device takes work items (tiles, in tile_order) from
+     * it until none is left.  NULL: one CTA per work item. */
+    uint32_t* work_queue;
 } tg_raster_fwd_args;
 TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
 

@@ -41,12 +41,12 @@ def leaves(cat):
     return {k: T(v).requires_grad_() for k, v in cat.items()}
 
 
-def run_batch(cat, offs, V, K, vs, textured=True, mode="RGB", tile=16, order="heaviest_first"):
+def run_batch(cat, offs, V, K, vs, textured=True, mode="RGB", tile=16, order="heaviest_first", persistent=False):
     L = leaves(cat)
     out = rasterization_textured_gaussians_batch(
         L["means"], L["quats"], L["scales"], L["opacities"], L["colors"], L["textures"] if textured else None, offs,
         T(V), T(K), [w for w, _ in SIZES], [h for _, h in SIZES], vs, sh_degree=0, tile_size=tile, render_mode=mode,
-        far_plane=100.0, tile_order=order)
+        far_plane=100.0, tile_order=order, persistent=persistent)
     return out, L
 
 
@@ -71,10 +71,11 @@ def loss_weights(shapes, seed=4):
     return [T(rng.normal(size=s)) for s in shapes]
 
 
-@pytest.mark.parametrize("textured,mode,tile", [(True, "RGB", 16), (True, "RGB+ED", 8), (False, "RGB", 16)])
-def test_batch_matches_per_view_calls(textured, mode, tile):
+@pytest.mark.parametrize("textured,mode,tile,persistent", [(True, "RGB", 16, False), (True, "RGB+ED", 8, False),
+                                                           (False, "RGB", 16, False), (True, "RGB", 8, True)])
+def test_batch_matches_per_view_calls(textured, mode, tile, persistent):
     cat, offs, V, K, vs = make_batch()
-    bo, bl = run_batch(cat, offs, V, K, vs, textured, mode, tile)
+    bo, bl = run_batch(cat, offs, V, K, vs, textured, mode, tile, persistent=persistent)
     po, pl = run_per_view(cat, offs, V, K, vs, textured, mode, tile)
     for c in range(len(SIZES)):
         ref = po[c]

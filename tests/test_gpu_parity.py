@@ -223,7 +223,7 @@ def test_plain_forward(name):
     _compare_fwd(g, o, 1e-4)
 
 
-def _grads_gpu(s, d, textured, filtering, bg=None, absgrad=False, seed=3, depth=0):
+def _grads_gpu(s, d, textured, filtering, bg=None, absgrad=False, seed=3, depth=0, persistent=False):
     rng = np.random.default_rng(seed)
     C, H, W = d["C"], s.height, s.width
     up = dict(c=rng.normal(size=(C, H, W, 3)), a=rng.normal(size=(C, H, W, 1)), n=rng.normal(size=(C, H, W, 3)),
@@ -239,10 +239,12 @@ def _grads_gpu(s, d, textured, filtering, bg=None, absgrad=False, seed=3, depth=
     if textured:
         out = rasterize_to_pixels_textured_gaussians(
             m2d, M, cols, opac, tex, 3.0, 3.0, nrm, dens, W, H, s.tile_size, d["off"], d["fl"],
-            backgrounds=None if bg is None else T(bg), absgrad=absgrad, filtering=filtering, batch_depth=depth)
+            backgrounds=None if bg is None else T(bg), absgrad=absgrad, filtering=filtering, batch_depth=depth,
+            persistent=persistent)
     else:
         out = rasterize_to_pixels_2dgs(m2d, M, cols, opac, nrm, dens, W, H, s.tile_size, d["off"], d["fl"],
-                                       backgrounds=None if bg is None else T(bg), absgrad=absgrad, batch_depth=depth)
+                                       backgrounds=None if bg is None else T(bg), absgrad=absgrad, batch_depth=depth,
+                                       persistent=persistent)
     loss = ((out[0] * T(up["c"])).sum() + (out[1] * T(up["a"])).sum() + (out[2] * T(up["n"])).sum()
             + (out[3] * T(up["d"])).sum() + (out[4] * T(up["m"])).sum())
     loss.backward()
@@ -391,4 +393,20 @@ def test_batch_depth_changes_nothing(tile, depth):
     for a, b in zip(out0[:5], out1[:5]):  # per-pixel outputs (the statistics are float atomics)
         assert torch.equal(a, b)
     for k in ("means2d", "M", "colors", "opac", "normals", "textures", "densify"):
+        assert rel_l2(to_np(g1[k]), to_np(g0[k])) < 1e-6, k
+
+
+@pytest.mark.parametrize("tile,textured", [(8, True), (16, True), (32, True), (16, False)])
+def test_persistent_launch_changes_nothing(tile, textured):
+    """CTAs taking tiles from a device work counter compute every tile exactly as one CTA per tile does."""
+    s = scenes.small()
+    s.tile_size = tile
+    d = _raster_inputs(s)
+    f = "bilinear" if textured else None
+    g0, _, out0 = _grads_gpu(s, d, textured, f)
+    g1, _, out1 = _grads_gpu(s, d, textured, f, persistent=True)
+    for a, b in zip(out0[:5], out1[:5]):
+        assert torch.equal(a, b)
+    assert torch.equal(out0[6], out1[6])  # contribution counts
+    for k in ("means2d", "M", "colors", "opac", "normals", "densify") + (("textures",) if textured else ()):
         assert rel_l2(to_np(g1[k]), to_np(g0[k])) < 1e-6, k

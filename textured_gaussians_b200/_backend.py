@@ -70,7 +70,7 @@ class RasterFwdArgs(ctypes.Structure):
                 ("out_colors", P), ("out_alphas", P), ("out_normals", P), ("out_distort", P), ("out_median", P),
                 ("last_ids", P), ("median_ids", P), ("contrib_sum", P), ("contrib_count", P), ("tile_order", P),
                 ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64), ("n_isects_dev", P),
-                ("batch_depth", I32)]
+                ("batch_depth", I32), ("work_queue", P)]
 
 
 class RasterBwdArgs(ctypes.Structure):

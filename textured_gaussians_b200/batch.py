@@ -132,6 +132,7 @@ def rasterization_textured_gaussians_batch(
     tile_order: str = "heaviest_first",
     view_table: Optional[ViewTable] = None,
     batch_depth: int = 0,
+    persistent: bool = False,
 ):
     """Render C views of uneven size, view c showing scene ``view_scenes[c]``.
 
@@ -185,7 +186,8 @@ def rasterization_textured_gaussians_batch(
              else None)
 
     common = dict(backgrounds=backgrounds, packed=True, absgrad=absgrad, gs_contrib_threshold=gs_contrib_threshold,
-                  gaussian_ids=gaussian_ids, tile_order=order, view_table=vt, batch_depth=batch_depth)
+                  gaussian_ids=gaussian_ids, tile_order=order, view_table=vt, batch_depth=batch_depth,
+                  persistent=persistent)
     if textures is not None:
         if filtering not in _FILTER_ADJOINT:
             raise Exception(f"Unsupported filter type {filtering}")

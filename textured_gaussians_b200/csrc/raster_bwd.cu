@@ -198,10 +198,10 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
     P.buf_n[2] += nn.z * fac;
 }
 
+// One work item (tile) of the adjoint; every early return is uniform over the CTA.
 template <int D, class Tex, int PPT>
-__global__ void __launch_bounds__(256, BwdBounds<PPT>::kMinCtas) raster_bwd_kernel(const tg_raster_bwd_args a,
-                                                                                   const float uv_scale,
-                                                                                   const int bs) {
+__device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const float uv_scale, const int bs,
+                                         const int64_t item) {
     using GS = GradSlots<D>;
     constexpr int NV = GS::kCount;
     const tg_raster_fwd_args& f = a.f;
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(256, BwdBounds<PPT>::kMinCtas) raster_bwd_kern
     __shared__ int s_max_bin;
 
     const unsigned wmask = __activemask();
-    const TileWork tc = tile_work(f, blockIdx.x);
+    const TileWork tc = tile_work(f, item);
     if (!tc.valid) return;  // uniform over the CTA
     const int tr = threadIdx.x, lane = tr & 31;
     if (f.masks != nullptr && !f.masks[tc.t]) return;
@@ -373,6 +373,30 @@ __global__ void __launch_bounds__(256, BwdBounds<PPT>::kMinCtas) raster_bwd_kern
     }
 }
 
+// CTA per work item, or (work_queue != NULL) a persistent grid whose CTAs take
+// items from the queue counter until none is left.
+template <int D, class Tex, int PPT, bool kPersistent>
+__global__ void __launch_bounds__(256, BwdBounds<PPT>::kMinCtas) raster_bwd_kernel(const tg_raster_bwd_args a,
+                                                                                   const float uv_scale,
+                                                                                   const int bs,
+                                                                                   const int64_t n_items) {
+    if constexpr (!kPersistent) {
+        bwd_tile<D, Tex, PPT>(a, uv_scale, bs, blockIdx.x);
+        return;
+    }
+    else {
+        __shared__ int64_t s_item;
+        for (;;) {
+            if (threadIdx.x == 0) s_item = (int64_t)atomicAdd(a.f.work_queue, 1u);
+            __syncthreads();  // also: every thread is done with the previous item's shared memory
+            const int64_t item = s_item;
+            __syncthreads();  // s_item read by all before it is rewritten
+            if (item >= n_items) return;
+            bwd_tile<D, Tex, PPT>(a, uv_scale, bs, item);
+        }
+    }
+}
+
 // v_densify[e] = (v_M[e][2], v_M[e][5]) * M[e][8], once every contribution is in.
 __global__ void densify_grad_kernel(const float* __restrict__ v_M, const float* __restrict__ M, int64_t n,
                                     float* __restrict__ v_densify) {
@@ -396,16 +420,25 @@ cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     const int64_t blocks = f.views ? f.n_tiles : (int64_t)f.C * f.tile_width * f.tile_height;
     const float uv_scale = a.adjoint == TG_ADJ_BWD2 ? 1.f : (a.adjoint == TG_ADJ_EXACT ? 0.5f : 0.f);
     const bool four = tile_px > 256;  // 32x32 tiles: four pixels per thread, 256 threads
-    cudaError_t err = four ? cudaFuncSetAttribute(raster_bwd_kernel<D, Tex, 4>,
-                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                           : cudaFuncSetAttribute(raster_bwd_kernel<D, Tex, 1>,
-                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const bool pers = f.work_queue != nullptr;
+    const void* fn = four ? (pers ? (const void*)raster_bwd_kernel<D, Tex, 4, true>
+                                  : (const void*)raster_bwd_kernel<D, Tex, 4, false>)
+                          : (pers ? (const void*)raster_bwd_kernel<D, Tex, 1, true>
+                                  : (const void*)raster_bwd_kernel<D, Tex, 1, false>);
+    const int threads = four ? tile_px / 4 : tile_px;
+    cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     if (blocks > 0 && f.n_isects > 0) {
-        if (four)
-            raster_bwd_kernel<D, Tex, 4><<<(unsigned)blocks, tile_px / 4, smem, s>>>(a, uv_scale, bs);
-        else
-            raster_bwd_kernel<D, Tex, 1><<<(unsigned)blocks, tile_px, smem, s>>>(a, uv_scale, bs);
+        int64_t grid = blocks;
+        if (pers) {
+            if ((err = cudaMemsetAsync(f.work_queue, 0, sizeof(uint32_t), s)) != cudaSuccess) return err;
+            if ((err = persistent_grid(fn, threads, smem, blocks, grid)) != cudaSuccess) return err;
+        }
+        const dim3 g((unsigned)grid), b((unsigned)threads);
+        if (four && pers) raster_bwd_kernel<D, Tex, 4, true><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        else if (four) raster_bwd_kernel<D, Tex, 4, false><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        else if (pers) raster_bwd_kernel<D, Tex, 1, true><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        else raster_bwd_kernel<D, Tex, 1, false><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
         note_launches(1);
     }
     if ((err = cudaGetLastError()) != cudaSuccess) return err;

@@ -230,4 +230,16 @@ __device__ __forceinline__ int64_t pixel_index(const TileWork& w, int i, int j) 
     return (p >= 0 && p < w.pix_limit) ? p : -1;
 }
 
+// Grid of a persistent launch: every CTA that fits on the device at once, at
+// most one per work item.
+inline cudaError_t persistent_grid(const void* fn, int threads, size_t smem, int64_t n_items, int64_t& grid) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+    if (e != cudaSuccess) return e;
+    grid = std::min<int64_t>(n_items, (int64_t)std::max(sms, 1) * std::max(per_sm, 1));
+    return cudaSuccess;
+}
+
 }  // namespace tg

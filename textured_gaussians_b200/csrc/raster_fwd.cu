@@ -34,9 +34,9 @@ struct FwdBounds {
     static constexpr int kMinCtas = PPT == 1 ? TG_FWD_MIN_CTAS : 1;
 };
 
+// One work item (tile) of the forward; every early return is uniform over the CTA.
 template <int D, class Tex, int PPT>
-__global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kernel(const tg_raster_fwd_args a,
-                                                                                   const int bs) {
+__device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int bs, const int64_t item) {
     constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
     extern __shared__ float4 smem4[];
     const int nt = blockDim.x;  // threads: tile_size^2 / PPT; bs = splats staged per batch
@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kern
     int* s_row = reinterpret_cast<int*>(s_col + bs * D);
 
     const unsigned wmask = __activemask();
-    const TileWork tc = tile_work(a, blockIdx.x);
+    const TileWork tc = tile_work(a, item);
     if (!tc.valid) return;  // uniform over the CTA
     const int tr = threadIdx.x, lane = tr & 31;
     const int ts = a.tile_size;
@@ -221,6 +221,29 @@ __global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kern
     }
 }
 
+// CTA per work item, or (work_queue != NULL) a persistent grid whose CTAs take
+// items from the queue counter until none is left.
+template <int D, class Tex, int PPT, bool kPersistent>
+__global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kernel(const tg_raster_fwd_args a,
+                                                                                   const int bs,
+                                                                                   const int64_t n_items) {
+    if constexpr (!kPersistent) {
+        fwd_tile<D, Tex, PPT>(a, bs, blockIdx.x);
+        return;
+    }
+    else {
+        __shared__ int64_t s_item;
+        for (;;) {
+            if (threadIdx.x == 0) s_item = (int64_t)atomicAdd(a.work_queue, 1u);
+            __syncthreads();  // also: every thread is done with the previous item's shared memory
+            const int64_t item = s_item;
+            __syncthreads();  // s_item read by all before it is rewritten
+            if (item >= n_items) return;
+            fwd_tile<D, Tex, PPT>(a, bs, item);
+        }
+    }
+}
+
 size_t fwd_smem_bytes(int D, int bs) { return (size_t)bs * (6 * sizeof(float4) + D * sizeof(float) + sizeof(int)); }
 
 template <int D, class Tex>
@@ -230,18 +253,25 @@ cudaError_t launch_fwd_t(const tg_raster_fwd_args& a, cudaStream_t s) {
     const size_t smem = fwd_smem_bytes(D, bs);
     const int64_t blocks = a.views ? a.n_tiles : (int64_t)a.C * a.tile_width * a.tile_height;
     if (blocks == 0) return cudaSuccess;
-    cudaError_t err;
-    if (tile_px > 256) {  // 32x32 tiles: four pixels per thread, 256 threads
-        err = cudaFuncSetAttribute(raster_fwd_kernel<D, Tex, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem);
-        if (err != cudaSuccess) return err;
-        raster_fwd_kernel<D, Tex, 4><<<(unsigned)blocks, tile_px / 4, smem, s>>>(a, bs);
-    } else {
-        err = cudaFuncSetAttribute(raster_fwd_kernel<D, Tex, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem);
-        if (err != cudaSuccess) return err;
-        raster_fwd_kernel<D, Tex, 1><<<(unsigned)blocks, tile_px, smem, s>>>(a, bs);
+    const bool four = tile_px > 256;  // 32x32 tiles: four pixels per thread, 256 threads
+    const bool pers = a.work_queue != nullptr;
+    const void* fn = four ? (pers ? (const void*)raster_fwd_kernel<D, Tex, 4, true>
+                                  : (const void*)raster_fwd_kernel<D, Tex, 4, false>)
+                          : (pers ? (const void*)raster_fwd_kernel<D, Tex, 1, true>
+                                  : (const void*)raster_fwd_kernel<D, Tex, 1, false>);
+    const int threads = four ? tile_px / 4 : tile_px;
+    cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    int64_t grid = blocks;
+    if (pers) {
+        if ((err = cudaMemsetAsync(a.work_queue, 0, sizeof(uint32_t), s)) != cudaSuccess) return err;
+        if ((err = persistent_grid(fn, threads, smem, blocks, grid)) != cudaSuccess) return err;
     }
+    const dim3 g((unsigned)grid), b((unsigned)threads);
+    if (four && pers) raster_fwd_kernel<D, Tex, 4, true><<<g, b, smem, s>>>(a, bs, blocks);
+    else if (four) raster_fwd_kernel<D, Tex, 4, false><<<g, b, smem, s>>>(a, bs, blocks);
+    else if (pers) raster_fwd_kernel<D, Tex, 1, true><<<g, b, smem, s>>>(a, bs, blocks);
+    else raster_fwd_kernel<D, Tex, 1, false><<<g, b, smem, s>>>(a, bs, blocks);
     note_launches(1);
     return cudaGetLastError();
 }

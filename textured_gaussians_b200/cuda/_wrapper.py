@@ -540,7 +540,8 @@ def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_stor
         None if layout is None else B.ptr(layout.get("tile_order")),
         None if vt is None else B.ptr(vt.views), None if vt is None else B.ptr(vt.tile_view),
         0 if vt is None else vt.n_tiles, 0 if vt is None else vt.n_pixels, B.ptr(n_isects_dev),
-        0 if layout is None else layout.get("batch_depth", 0))
+        0 if layout is None else layout.get("batch_depth", 0),
+        None if layout is None else B.ptr(layout.get("work_queue")))
 
 
 class _RasterizeToPixelsTextured(torch.autograd.Function):
@@ -649,12 +650,14 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
                 None)
 
 
-def _layout(tile_order, view_table, batch_depth=0):
-    if tile_order is None and view_table is None and not batch_depth:
+def _layout(tile_order, view_table, batch_depth=0, persistent=False, device=None):
+    if tile_order is None and view_table is None and not batch_depth and not persistent:
         return None
     if tile_order is not None:
         tile_order = tile_order.to(torch.int32).contiguous()
-    return {"tile_order": tile_order, "view_table": view_table, "batch_depth": int(batch_depth or 0)}
+    queue = torch.zeros((1,), dtype=torch.int32, device=device) if persistent else None
+    return {"tile_order": tile_order, "view_table": view_table, "batch_depth": int(batch_depth or 0),
+            "work_queue": queue}
 
 
 def _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
@@ -714,6 +717,7 @@ def rasterize_to_pixels_textured_gaussians(
     tile_order: Optional[Tensor] = None,
     view_table=None,
     batch_depth: int = 0,
+    persistent: bool = False,
 ) -> Tuple[Tensor, ...]:
     """Rasterize textured 2D Gaussians to pixels (reference: cuda/_wrapper.py:1806-2002).
 
@@ -735,6 +739,8 @@ def rasterize_to_pixels_textured_gaussians(
     flat ``isect_offsets`` from :func:`isect_offset_encode_views`, flat
     per-pixel outputs [n_pixels, ...]).  ``batch_depth`` sets how many splats
     are staged in shared memory per batch (0: tile_size^2, the reference's).
+    ``persistent=True`` launches as many CTAs as fit on the device, which take
+    tiles from a device work counter instead of one CTA per tile.
     """
     _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
                   backgrounds, packed, view_table)
@@ -763,7 +769,7 @@ def rasterize_to_pixels_textured_gaussians(
         float(texture_range_x), float(texture_range_y), int(image_width), int(image_height), int(tile_size),
         isect_offsets.contiguous(), flatten_ids.contiguous(), absgrad, gs_contrib_threshold, g_weight,
         _FILTER_ADJOINT[filtering], False, gaussian_ids, textures.shape[0],
-        _layout(tile_order, view_table, batch_depth))
+        _layout(tile_order, view_table, batch_depth, persistent, means2d.device))
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]
@@ -794,6 +800,7 @@ def rasterize_to_pixels_2dgs(
     tile_order: Optional[Tensor] = None,
     view_table=None,
     batch_depth: int = 0,
+    persistent: bool = False,
 ) -> Tuple[Tensor, ...]:
     """Rasterize plain 2D Gaussians to pixels (reference: cuda/_wrapper.py:1647-1784).
 
@@ -802,7 +809,7 @@ def rasterize_to_pixels_2dgs(
     Packed inputs: the contribution statistics are per entry, [nnz], or per
     Gaussian, [n_gaussians], when ``gaussian_ids`` and ``n_gaussians`` are
     given (the reference sizes them [0] for packed inputs).  ``tile_order``,
-    ``view_table`` and ``batch_depth`` as in
+    ``view_table``, ``batch_depth`` and ``persistent`` as in
     :func:`rasterize_to_pixels_textured_gaussians`.
     """
     _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
@@ -821,7 +828,7 @@ def rasterize_to_pixels_2dgs(
         normals.contiguous(), densify.contiguous(), None if backgrounds is None else backgrounds.contiguous(), masks,
         None, None, 3.0, 3.0, int(image_width), int(image_height), int(tile_size), isect_offsets.contiguous(),
         flatten_ids.contiguous(), absgrad, gs_contrib_threshold, 1.0, B.TG_ADJ_REFERENCE, True, gaussian_ids,
-        int(n_gaussians), _layout(tile_order, view_table, batch_depth))
+        int(n_gaussians), _layout(tile_order, view_table, batch_depth, persistent, means2d.device))
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]

@@ -18,7 +18,8 @@ Extensions (keyword-only, default off): ``texture_storage`` /
 adjoint end to end), ``tile_order`` ("heaviest_first", the default: compositor
 tiles taken by descending intersection count, so the longest tiles do not form
 the launch's tail; "launch": tile index order; the results are the same),
-``batch_depth`` (splats staged per compositor batch; 0 = tile_size^2) and
+``batch_depth`` (splats staged per compositor batch; 0 = tile_size^2),
+``persistent`` (compositor CTAs take tiles from a device work counter) and
 ``tile_size`` 32 besides the reference's 8 and 16.
 """
 from __future__ import annotations
@@ -185,6 +186,7 @@ def rasterization_2dgs(
     adjoint: str = "reference",
     tile_order: str = "heaviest_first",
     batch_depth: int = 0,
+    persistent: bool = False,
 ) -> Tuple[Tensor, Tensor, Tensor, Optional[Tensor], Tensor, Tensor, Tensor, Tensor, Dict]:
     """Rasterize 2D Gaussian surfels (N) to C image planes (reference: rendering.py:1009-1338).
 
@@ -199,7 +201,8 @@ def rasterization_2dgs(
         p["means2d"], p["ray_transforms"], p["colors"], p["opacities"], p["normals"], p["densify"], width, height,
         tile_size, p["isect_offsets"], p["flatten_ids"], backgrounds=backgrounds, packed=packed, absgrad=absgrad,
         distloss=distloss, gs_contrib_threshold=gs_contrib_threshold, gaussian_ids=p["gaussian_ids"],
-        n_gaussians=means.shape[0] if packed else None, tile_order=p["tile_order"], batch_depth=batch_depth)
+        n_gaussians=means.shape[0] if packed else None, tile_order=p["tile_order"], batch_depth=batch_depth,
+        persistent=persistent)
     return _finish(p, *outs, viewmats, Ks, width, height, tile_size, render_mode, depth_mode)
 
 
@@ -239,6 +242,7 @@ def rasterization_textured_gaussians(
     adjoint: str = "reference",
     tile_order: str = "heaviest_first",
     batch_depth: int = 0,
+    persistent: bool = False,
 ) -> Tuple[Tensor, Tensor, Tensor, Optional[Tensor], Tensor, Tensor, Tensor, Tensor, Dict]:
     """Rasterize textured 2D Gaussian surfels (reference: rendering.py:1342-1685).
 
@@ -257,5 +261,6 @@ def rasterization_textured_gaussians(
         backgrounds=backgrounds, packed=packed, absgrad=absgrad, distloss=distloss,
         gs_contrib_threshold=gs_contrib_threshold, filtering=filtering, g_weight=g_weight,
         texture_storage=texture_storage, texture_scales=texture_scales, gaussian_ids=p["gaussian_ids"],
-        tile_order=p["tile_order"], batch_depth=batch_depth)
+        tile_order=p["tile_order"], batch_depth=batch_depth,
+        persistent=persistent)
     return _finish(p, *outs, viewmats, Ks, width, height, tile_size, render_mode, depth_mode)
