@@ -18,6 +18,11 @@ Arms:
       the CPU oracle (this repository's C++ restatement of the reference
       kernels, OpenMP on all host cores) on a bounded tile sample.
 
+Timing: CUDA events on the bench's stream; inputs (textures 8.4 GB BF16 /
+16.8 GB FP32) exceed the 126 MB L2; Python's cyclic GC is paused inside timed
+loops (each step reads the intersection count back once, as the reference
+does, so a host pause would show up as GPU idle time).
+
 Multi-GPU (torchrun): every rank renders its own four cameras of the same
 scene (replicas, weak scaling); time = max over ranks, value = all pixels /
 time.  Prints one JSON line on rank 0.
@@ -25,6 +30,8 @@ time.  Prints one JSON line on rank 0.
 from __future__ import annotations
 
 import argparse
+import contextlib
+import gc
 import json
 import math
 import os
@@ -92,6 +99,20 @@ def gpu_textures(n_splats, R, device, seed=3):
         a = torch.randn((n, 4, 4, 4), generator=g, device=device) * 0.3
         out[s:s + n] = (0.5 + torch.einsum("yv,xu,nvuc->nyxc", basis, basis, a)).clamp_(0.0, 1.0)
     return out
+
+
+@contextlib.contextmanager
+def no_gc():
+    """Python's cyclic GC paused for a timed loop (collected just before): each step waits once on the host for
+    the intersection count, so a host-side GC pause would otherwise show up as GPU idle time."""
+    gc.collect()
+    was = gc.isenabled()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if was:
+            gc.enable()
 
 
 # ---------------------------------------------------------------- clocks
@@ -257,13 +278,14 @@ def _run_ours(args, rank, world, local, dev):
         t1 = torch.cuda.Event(enable_timing=True)
         l0 = B.lib().tg_kernel_launch_count()
         B.TIMERS.enable(True)
-        t0.record()
-        for i in range(steps):
-            starts[i].record()
-            out, _ = step(storage, tile_size, per_view, depth)
-            ends[i].record()
-        t1.record()
-        torch.cuda.synchronize()
+        with no_gc():
+            t0.record()
+            for i in range(steps):
+                starts[i].record()
+                out, _ = step(storage, tile_size, per_view, depth)
+                ends[i].record()
+            t1.record()
+            torch.cuda.synchronize()
         launches = B.lib().tg_kernel_launch_count() - l0
         stages = B.TIMERS.summary()
         B.TIMERS.enable(False)
@@ -357,11 +379,12 @@ def timed_plain(fn, steps, warmup=1):
     torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
-    t0.record()
-    for _ in range(steps):
-        fn()
-    t1.record()
-    torch.cuda.synchronize()
+    with no_gc():
+        t0.record()
+        for _ in range(steps):
+            fn()
+        t1.record()
+        torch.cuda.synchronize()
     return t0.elapsed_time(t1) / steps
 
 
@@ -376,11 +399,12 @@ def time_graphed(fn, steps, pixels):
     torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
-    t0.record()
-    for _ in range(steps):
-        g.replay()
-    t1.record()
-    torch.cuda.synchronize()
+    with no_gc():
+        t0.record()
+        for _ in range(steps):
+            g.replay()
+        t1.record()
+        torch.cuda.synchronize()
     ms = t0.elapsed_time(t1) / steps
     over = g.overflowed()
     out = {"value": round(pixels / (ms / 1e3) / 1e6, 2), "unit": "Mpix/s", "ms_per_step": round(ms, 3),
@@ -609,11 +633,12 @@ def _run_batch(args, dev):
         t1 = torch.cuda.Event(enable_timing=True)
         l0 = B.lib().tg_kernel_launch_count()
         B.TIMERS.enable(True)
-        t0.record()
-        for _ in range(steps):
-            fn()
-        t1.record()
-        torch.cuda.synchronize()
+        with no_gc():
+            t0.record()
+            for _ in range(steps):
+                fn()
+            t1.record()
+            torch.cuda.synchronize()
         stages = {k: round(statistics.mean(v), 3) for k, v in B.TIMERS.summary().items()}
         B.TIMERS.enable(False)
         return t0.elapsed_time(t1) / steps, stages, B.lib().tg_kernel_launch_count() - l0

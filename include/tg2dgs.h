@@ -89,6 +89,13 @@ typedef struct {
     float* depths;         /* [C,N] */
     float* ray_transforms; /* [C,N,3,3] rows of K*[R*s0*q0, R*s1*q1, mean_c] */
     float* normals;        /* [C,N,3] */
+    /* Fused SH colours (sh_coeffs NULL: not computed), replacing the
+     * reference's spherical_harmonics + clamp glue (rendering.py:1573-1583):
+     * colors[c,n] = max(SH(sh_degree, mean_n - centre_c) + 0.5, 0) for visible
+     * entries, 0.5 elsewhere; centre_c = -R_c^-1 t_c from viewmats[c]. */
+    int32_t sh_degree, sh_K;     /* degree <= 4, (degree+1)^2 <= K */
+    const float* sh_coeffs;      /* [N,K,3] */
+    float* colors;               /* [C,N,3] */
 } tg_project_fwd_args;
 TG_API int tg_project_fwd(const tg_project_fwd_args* a, tg_stream_t stream);
 
@@ -113,6 +120,13 @@ typedef struct {
     float* v_means;  /* [N,3] */
     float* v_quats;  /* [N,4] */
     float* v_scales; /* [N,3] */
+    /* Fused SH adjoint (sh_coeffs NULL: none): v_colors [C,N,3] in;
+     * v_sh_coeffs [N,K,3] out (overwritten); the direction's gradient is
+     * added into v_means. */
+    int32_t sh_degree, sh_K;
+    const float* sh_coeffs;
+    const float* v_colors;
+    float* v_sh_coeffs;
 } tg_project_bwd_args;
 TG_API int tg_project_bwd(const tg_project_bwd_args* a, tg_stream_t stream);
 
@@ -162,6 +176,10 @@ typedef struct {
      * min(*nnz, capacity) entries and sets *overflow to 1 if *nnz > capacity.
      * The caller zeroes *overflow. */
     uint32_t* overflow;
+    /* Fused SH colours as in tg_project_fwd_args (emit): colors [nnz,3]. */
+    int32_t sh_degree, sh_K;
+    const float* sh_coeffs;
+    float* colors;
 } tg_project_packed_args;
 TG_API size_t tg_project_packed_workspace_bytes(int32_t C, int32_t N);
 TG_API int tg_project_packed_count(const tg_project_packed_args* a, tg_stream_t stream);
@@ -193,6 +211,14 @@ typedef struct {
     float* v_means;
     float* v_quats;
     float* v_scales;
+    /* Fused SH adjoint as in tg_project_bwd_args: v_colors [nnz,3] in;
+     * v_sh_coeffs [N,K,3] out (zeroed, then accumulated with atomics); the
+     * direction's gradient is added into v_means (the entry's row when
+     * sparse_grad). */
+    int32_t sh_degree, sh_K;
+    const float* sh_coeffs;
+    const float* v_colors;
+    float* v_sh_coeffs;
 } tg_project_packed_bwd_args;
 TG_API int tg_project_packed_bwd(const tg_project_packed_bwd_args* a, tg_stream_t stream);
 

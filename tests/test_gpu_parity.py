@@ -410,3 +410,110 @@ def test_persistent_launch_changes_nothing(tile, textured):
     assert torch.equal(out0[6], out1[6])  # contribution counts
     for k in ("means2d", "M", "colors", "opac", "normals", "densify") + (("textures",) if textured else ()):
         assert rel_l2(to_np(g1[k]), to_np(g0[k])) < 1e-6, k
+
+
+def _near_degenerate_splats(n=4000, seed=0):
+    """Large splats close to the camera whose plane passes near the camera centre:
+    s0^2 t1z^2 + s1^2 t2z^2 = z^2 (1 + eps), eps in +-[1e-7, 1e-1] (log-uniform), so the
+    projection's `distance` cancels to a relative 1e-7..1e-1 of its terms."""
+    rng = np.random.default_rng(seed)
+    means, quats, scales = [], [], []
+    while len(means) < n:
+        mean = np.array([rng.uniform(-0.5, 0.5), rng.uniform(-0.5, 0.5), rng.uniform(0.5, 2.0)])
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        t1z, t2z = 2 * (x * z - w * y), 2 * (y * z + w * x)
+        if abs(t1z) < 0.3:
+            continue
+        eps = 10 ** rng.uniform(-7, -1) * rng.choice([-1, 1])
+        s1 = abs(rng.normal(0.1, 0.05))
+        rem = mean[2] ** 2 * (1 + eps) - (s1 * t2z) ** 2
+        if rem <= 0:
+            continue
+        means.append(mean)
+        quats.append(q)
+        scales.append([np.sqrt(rem) / abs(t1z), s1, s1])
+    f = lambda a: np.asarray(a, np.float32)
+    return f(means), f(quats), f(scales)
+
+
+def test_near_degenerate_projection_is_solved_in_fp64():
+    """Where the FP32 solve cancels (the IEEE-FP32 oracle is off by up to ~1e-2 relative and flips most radii),
+    the GPU's FP64 step matches the FP64 oracle to FP32 output rounding."""
+    means, quats, scales = _near_degenerate_splats()
+    V = np.eye(4, dtype=np.float32)[None]
+    K = np.array([[[1200, 0, 800], [0, 1200, 600], [0, 0, 1]]], np.float32)
+    radii, m2d, depths, M, nrm = fully_fused_projection_2dgs(T(means), T(quats), T(scales), T(V), T(K), 1600, 1200,
+                                                             0.3, 0.01, 100.0, 0.0)
+    r64, m64, d64, M64, n64 = O.project_fwd(means, quats, scales, V, K, 1600, 1200, 0.01, 100.0, dtype=F64)
+    r32, m32, _, _, _ = O.project_fwd(means, quats, scales, V, K, 1600, 1200, 0.01, 100.0, dtype=np.float32)
+    Mo = M64[0]
+    rel = np.abs(Mo[:, 2, 0] ** 2 + Mo[:, 2, 1] ** 2 - Mo[:, 2, 2] ** 2) / (Mo[:, 2] ** 2).sum(1)
+    deg = rel < 1.0 / 128  # safely inside the FP64 branch
+    radii = radii.cpu().numpy()[0]
+    # radii the oracle represents (its float -> int32 conversion of larger values is undefined in C++)
+    vis = deg & (r64[0] > 0) & (r64[0] < (1 << 30))
+    assert vis.sum() > 1000
+    assert (radii[vis] == r64[0][vis]).mean() > 0.99
+    both = vis & (radii > 0)
+    g = to_np(m2d)[0][both]
+    ref = m64[0][both]
+    err = np.abs(g - ref).max(1) / (np.abs(ref).max(1) + 1)
+    assert err.max() < 1e-6, err.max()
+    e32 = np.abs(m32[0][both] - ref).max(1) / (np.abs(ref).max(1) + 1)
+    assert e32.max() > 1e-4  # the FP32 chain really has cancelled on this set
+    assert_close(to_np(M)[0][both], M64[0][both], 1e-6 * np.abs(M64[0][both]).max(), 1e-6, 0, "ray transforms")
+
+
+def _sh_scene(seed=31, N=500, n_cams=3, K=16):
+    s = scenes.tiny(seed=seed, N=N, n_cams=n_cams)
+    rng = np.random.default_rng(seed)
+    sh = np.concatenate([rng.uniform(0, 1, size=(N, 1, 3)), rng.normal(0, 0.25, size=(N, K - 1, 3))], 1)
+    s.colors = sh.astype(np.float32)  # strong higher bands: some colours hit the clamp at 0
+    return s
+
+
+@pytest.mark.parametrize("packed", [False, True])
+def test_fused_sh_matches_unfused_path(packed):
+    """SH evaluated inside the projection (camera centre by cofactors in-kernel) against the separate SH op fed
+    by torch's inverse: images to 1e-5, gradients to 1e-5 relative, dense and packed."""
+    from textured_gaussians_b200 import rasterization_textured_gaussians
+
+    s = _sh_scene()
+    rng = np.random.default_rng(5)
+    w = T(rng.normal(size=(3, s.height, s.width, 3)))
+    res = []
+    for fuse in (True, False):
+        L = [T(x).requires_grad_() for x in (s.means, s.quats, s.scales, s.opacities, s.colors, s.textures)]
+        out = rasterization_textured_gaussians(*L, T(s.viewmats), T(s.Ks), s.width, s.height, sh_degree=3,
+                                               far_plane=s.far_plane, packed=packed, fuse_sh=fuse)
+        (out[0] * w).sum().backward()
+        res.append((out, [t.grad.to_dense() if t.grad.is_sparse else t.grad for t in L]))
+    (of, gf), (ou, gu) = res
+    assert torch.allclose(of[0], ou[0], atol=1e-5, rtol=0)
+    assert torch.allclose(of[1], ou[1], atol=1e-6, rtol=0)
+    for name, a, b in zip(("means", "quats", "scales", "opacities", "sh", "textures"), gf, gu):
+        assert rel_l2(to_np(a), to_np(b)) < 1e-5, (name, rel_l2(to_np(a), to_np(b)))
+
+
+def test_fused_sh_degree3_end_to_end_matches_oracle_pipeline():
+    from textured_gaussians_b200 import rasterization_textured_gaussians
+
+    s = _sh_scene(seed=32)
+    L = [T(x).requires_grad_() for x in (s.means, s.quats, s.scales, s.opacities, s.colors, s.textures)]
+    out = rasterization_textured_gaussians(*L, T(s.viewmats), T(s.Ks), s.width, s.height, sh_degree=3,
+                                           far_plane=s.far_plane)
+    rng = np.random.default_rng(0)
+    vc = rng.normal(size=tuple(out[0].shape)).astype(np.float32)
+    (out[0] * T(vc)).sum().backward()
+    meta = out[-1]
+    proj = tuple(to_np(meta[k]) if k != "radii" else meta[k].cpu().numpy()
+                 for k in ("radii", "means2d", "depths", "ray_transforms", "normals"))
+    rc, ra, rn, cache = P.render(s.means, s.quats, s.scales, s.opacities, s.colors, s.textures, s.viewmats, s.Ks,
+                                 s.width, s.height, sh_degree=3, far_plane=s.far_plane, proj_override=proj, dtype=F64)
+    assert_close(to_np(out[0]), rc, 1e-5, 1e-5, 1e-4, "colors")
+    g = P.render_backward(cache, s.means, s.quats, s.scales, s.opacities, s.colors, s.textures, s.viewmats, s.Ks,
+                          s.width, s.height, vc, sh_degree=3)
+    for nm, t in zip(("means", "quats", "scales", "opacities", "colors", "textures"), L):
+        assert rel_l2(to_np(t.grad), g[nm]) < 1e-4, (nm, rel_l2(to_np(t.grad), g[nm]))

@@ -29,13 +29,15 @@ F32 = ctypes.c_float
 class ProjectFwdArgs(ctypes.Structure):
     _fields_ = [("C", I32), ("N", I32), ("means", P), ("quats", P), ("scales", P), ("viewmats", P), ("Ks", P),
                 ("width", I32), ("height", I32), ("near_plane", F32), ("far_plane", F32), ("radius_clip", F32),
-                ("radii", P), ("means2d", P), ("depths", P), ("ray_transforms", P), ("normals", P)]
+                ("radii", P), ("means2d", P), ("depths", P), ("ray_transforms", P), ("normals", P),
+                ("sh_degree", I32), ("sh_K", I32), ("sh_coeffs", P), ("colors", P)]
 
 
 class ProjectBwdArgs(ctypes.Structure):
     _fields_ = [("C", I32), ("N", I32), ("means", P), ("quats", P), ("scales", P), ("viewmats", P), ("Ks", P),
                 ("radii", P), ("ray_transforms", P), ("v_means2d", P), ("v_depths", P), ("v_normals", P),
-                ("v_ray_transforms", P), ("mode", I32), ("v_means", P), ("v_quats", P), ("v_scales", P)]
+                ("v_ray_transforms", P), ("mode", I32), ("v_means", P), ("v_quats", P), ("v_scales", P),
+                ("sh_degree", I32), ("sh_K", I32), ("sh_coeffs", P), ("v_colors", P), ("v_sh_coeffs", P)]
 
 
 class ProjectPackedArgs(ctypes.Structure):
@@ -43,14 +45,16 @@ class ProjectPackedArgs(ctypes.Structure):
                 ("width", I32), ("height", I32), ("near_plane", F32), ("far_plane", F32), ("radius_clip", F32),
                 ("workspace", P), ("nnz", P), ("indptr", P), ("nnz_host", I64), ("camera_ids", P),
                 ("gaussian_ids", P), ("radii", P), ("means2d", P), ("depths", P), ("ray_transforms", P),
-                ("normals", P), ("views", P), ("gauss_ranges", P), ("max_range", I32), ("overflow", P)]
+                ("normals", P), ("views", P), ("gauss_ranges", P), ("max_range", I32), ("overflow", P),
+                ("sh_degree", I32), ("sh_K", I32), ("sh_coeffs", P), ("colors", P)]
 
 
 class ProjectPackedBwdArgs(ctypes.Structure):
     _fields_ = [("C", I32), ("N", I32), ("nnz", I64), ("means", P), ("quats", P), ("scales", P), ("viewmats", P),
                 ("Ks", P), ("camera_ids", P), ("gaussian_ids", P), ("ray_transforms", P), ("v_means2d", P),
                 ("v_depths", P), ("v_normals", P), ("v_ray_transforms", P), ("mode", I32), ("sparse_grad", I32),
-                ("v_means", P), ("v_quats", P), ("v_scales", P)]
+                ("v_means", P), ("v_quats", P), ("v_scales", P), ("sh_degree", I32), ("sh_K", I32),
+                ("sh_coeffs", P), ("v_colors", P), ("v_sh_coeffs", P)]
 
 
 class IsectArgs(ctypes.Structure):

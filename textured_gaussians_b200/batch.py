@@ -133,6 +133,7 @@ def rasterization_textured_gaussians_batch(
     view_table: Optional[ViewTable] = None,
     batch_depth: int = 0,
     persistent: bool = False,
+    fuse_sh: bool = True,
 ):
     """Render C views of uneven size, view c showing scene ``view_scenes[c]``.
 
@@ -161,11 +162,16 @@ def rasterization_textured_gaussians_batch(
     ranges, max_range = vt.gauss_ranges(offs, view_scenes)
     mode = B.TG_ADJ_EXACT if adjoint == "exact" else (B.TG_ADJ_BWD2 if norm_rot_grad else B.TG_ADJ_REFERENCE)
 
-    camera_ids, gaussian_ids, radii, means2d, depths, ray_transforms, normals = _FullyFusedProjectionPacked2DGS.apply(
+    fuse = fuse_sh and sh_degree is not None
+    sh = (colors.float().contiguous(), int(sh_degree)) if fuse else (None, 0)
+    proj = _FullyFusedProjectionPacked2DGS.apply(
         means.contiguous(), quats.contiguous(), scales.contiguous(), viewmats.contiguous(), Ks.contiguous(), 0, 0,
-        eps2d, near_plane, far_plane, radius_clip, False, mode, (vt.views, ranges, max_range))
+        eps2d, near_plane, far_plane, radius_clip, False, mode, (vt.views, ranges, max_range), *sh)
+    camera_ids, gaussian_ids, radii, means2d, depths, ray_transforms, normals = proj[:7]
     opac = opacities[gaussian_ids]
-    if sh_degree is not None:
+    if fuse:
+        cols = proj[-1]
+    elif sh_degree is not None:
         camtoworlds = _inverse(viewmats)
         dirs = means[gaussian_ids, :] - camtoworlds[camera_ids, :3, 3]
         cols = spherical_harmonics(sh_degree, dirs, colors[gaussian_ids], masks=radii > 0)

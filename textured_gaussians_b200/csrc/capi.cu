@@ -89,6 +89,14 @@ int64_t raster_pixels(const tg_raster_fwd_args& a) {
     return a.views ? a.n_pixels : (int64_t)a.C * a.height * a.width;
 }
 
+int check_sh(int32_t degree, int32_t K, const float* coeffs, const void* out) {
+    if (coeffs == nullptr) return TG_OK;
+    TG_REQUIRE(degree >= 0 && degree <= 4 && (degree + 1) * (degree + 1) <= K && K <= 25, TG_ERR_INVALID_ARG,
+               "bad fused SH degree %d for %d bases", degree, K);
+    TG_REQUIRE(out != nullptr, TG_ERR_INVALID_ARG, "fused SH needs its output buffer");
+    return TG_OK;
+}
+
 int check_raster_common(const tg_raster_fwd_args& a) {
     TG_REQUIRE(a.C >= 0 && a.width >= 0 && a.height >= 0, TG_ERR_INVALID_ARG, "negative sizes");
     TG_REQUIRE(a.tile_size == 8 || a.tile_size == 16 || a.tile_size == 32, TG_ERR_UNSUPPORTED,
@@ -152,6 +160,8 @@ int tg_project_fwd(const tg_project_fwd_args* a, tg_stream_t stream) {
                TG_ERR_INVALID_ARG, "null pointer");
     TG_REQUIRE(aligned(a->quats, 16) && aligned(a->means2d, 8), TG_ERR_INVALID_ARG,
                "quats must be 16-byte and means2d 8-byte aligned");
+    const int rc = check_sh(a->sh_degree, a->sh_K, a->sh_coeffs, a->colors);
+    if (rc != TG_OK) return rc;
     return cuda_status(tg::launch_project_fwd(*a, stream), "tg_project_fwd");
 }
 
@@ -165,6 +175,9 @@ int tg_project_bwd(const tg_project_bwd_args* a, tg_stream_t stream) {
                    a->v_scales,
                TG_ERR_INVALID_ARG, "null pointer");
     TG_REQUIRE(aligned(a->quats, 16) && aligned(a->v_quats, 16), TG_ERR_INVALID_ARG, "quats must be 16-byte aligned");
+    int rc = check_sh(a->sh_degree, a->sh_K, a->sh_coeffs, a->v_sh_coeffs);
+    if (rc != TG_OK) return rc;
+    if (a->sh_coeffs) TG_REQUIRE(a->v_colors != nullptr, TG_ERR_INVALID_ARG, "fused SH adjoint needs v_colors");
     return cuda_status(tg::launch_project_bwd(*a, stream), "tg_project_bwd");
 }
 
@@ -201,6 +214,12 @@ int tg_project_packed_emit(const tg_project_packed_args* a, tg_stream_t stream) 
                    a->normals,
                TG_ERR_INVALID_ARG, "null output pointer");
     TG_REQUIRE(aligned(a->means2d, 8), TG_ERR_INVALID_ARG, "means2d must be 8-byte aligned");
+    const int rc_sh = check_sh(a->sh_degree, a->sh_K, a->sh_coeffs, a->colors);
+    if (rc_sh != TG_OK) return rc_sh;
+    if (a->sh_coeffs && a->overflow) {  // the unused tail's colours are zeroed (never rendered)
+        const cudaError_t e = cudaMemsetAsync(a->colors, 0, 12 * (size_t)a->nnz_host, stream);
+        if (e != cudaSuccess) return cuda_status(e, "tg_project_packed_emit memset");
+    }
     if (a->overflow) {  // capacity mode: every output zeroed, so the unused tail is inert
         const size_t n = (size_t)a->nnz_host;
         struct Z { void* p; size_t b; } zs[] = {{a->camera_ids, 8 * n}, {a->gaussian_ids, 8 * n}, {a->radii, 4 * n},
@@ -227,6 +246,13 @@ int tg_project_packed_bwd(const tg_project_packed_bwd_args* a, tg_stream_t strea
         if (e == cudaSuccess) e = cudaMemsetAsync(a->v_quats, 0, sizeof(float) * 4 * (size_t)rows, stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(a->v_scales, 0, sizeof(float) * 3 * (size_t)rows, stream);
         if (e != cudaSuccess) return cuda_status(e, "tg_project_packed_bwd");
+    }
+    const int rc_sh = check_sh(a->sh_degree, a->sh_K, a->sh_coeffs, a->v_sh_coeffs);
+    if (rc_sh != TG_OK) return rc_sh;
+    if (a->sh_coeffs && a->N > 0) {
+        TG_REQUIRE(a->v_colors != nullptr, TG_ERR_INVALID_ARG, "fused SH adjoint needs v_colors");
+        const cudaError_t e = cudaMemsetAsync(a->v_sh_coeffs, 0, sizeof(float) * 3 * a->sh_K * (size_t)a->N, stream);
+        if (e != cudaSuccess) return cuda_status(e, "tg_project_packed_bwd memset");
     }
     if (a->nnz == 0) return TG_OK;
     TG_REQUIRE(a->means && a->quats && a->scales && a->viewmats && a->Ks && a->camera_ids && a->gaussian_ids &&

@@ -2,7 +2,9 @@
 // camera-facing normal) and its adjoint, for sm_100a.
 //
 // Forward follows fully_fused_projection_2dgs_fwd.cu:58-238 of the reference
-// (same operation order, FP32); the adjoint follows
+// (same operation order, FP32), except that a near-degenerate transform (the
+// splat's plane through the camera centre, where the FP32 solve cancels) is
+// redone in FP64 from the FP32 parameters; the adjoint follows
 // fully_fused_projection_2dgs_bwd.cu:44-147 and utils.cuh:660-790, with a third,
 // exact form of the d(means2d)/d(ray transform) term.
 //
@@ -20,6 +22,7 @@
 // [C,N] intermediate; dense and packed share one device function, so a
 // packed entry is bit-identical to the dense entry it came from.
 #include "scan.cuh"
+#include "sh_eval.cuh"
 
 namespace tg {
 
@@ -31,6 +34,72 @@ struct Projected {
     float M[9];
     f3 nrm;
 };
+
+// The projection of Gaussian n into camera c entirely in FP64 from the FP32
+// parameters: taken only when the FP32 chain has cancelled (see project_one).
+// The same operations as project_one; outputs rounded to FP32 at the end.
+__device__ __noinline__ bool project_one_f64(const float* __restrict__ means, const float* __restrict__ quats,
+                                             const float* __restrict__ scales, const float* __restrict__ viewmats,
+                                             const float* __restrict__ Ks, int32_t width, int32_t height,
+                                             float near_plane, float far_plane, float radius_clip, int c, int64_t n,
+                                             Projected& o) {
+    const float* vm = viewmats + 16 * c;
+    double R[3][3], t[3], p[3], mc[3];
+    for (int r = 0; r < 3; ++r) {
+        for (int k = 0; k < 3; ++k) R[r][k] = (double)vm[4 * r + k];
+        t[r] = (double)vm[4 * r + 3];
+        p[r] = (double)means[3 * n + r];
+    }
+    for (int r = 0; r < 3; ++r) mc[r] = R[r][0] * p[0] + R[r][1] * p[1] + R[r][2] * p[2] + t[r];
+    if (mc[2] < (double)near_plane || mc[2] > (double)far_plane) return false;
+    double w = quats[4 * n], x = quats[4 * n + 1], y = quats[4 * n + 2], z = quats[4 * n + 3];
+    const double inv = 1.0 / sqrt(w * w + x * x + y * y + z * z);
+    w *= inv; x *= inv; y *= inv; z *= inv;
+    const double q0[3] = {1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y + w * z), 2.0 * (x * z - w * y)};
+    const double q1[3] = {2.0 * (x * y - w * z), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z + w * x)};
+    const double q2[3] = {2.0 * (x * z + w * y), 2.0 * (y * z - w * x), 1.0 - 2.0 * (x * x + y * y)};
+    const double s0 = scales[3 * n], s1 = scales[3 * n + 1];
+    double RS0[3], RS1[3], RS2[3];
+    for (int r = 0; r < 3; ++r) {
+        RS0[r] = s0 * (R[r][0] * q0[0] + R[r][1] * q0[1] + R[r][2] * q0[2]);
+        RS1[r] = s1 * (R[r][0] * q1[0] + R[r][1] * q1[1] + R[r][2] * q1[2]);
+        RS2[r] = R[r][0] * q2[0] + R[r][1] * q2[1] + R[r][2] * q2[2];
+    }
+    const float* K = Ks + 9 * c;
+    const double fx = K[0], cx = K[2], fy = K[4], cy = K[5];
+    const double M0[3] = {fx * RS0[0] + cx * RS0[2], fx * RS1[0] + cx * RS1[2], fx * mc[0] + cx * mc[2]};
+    const double M1[3] = {fy * RS0[1] + cy * RS0[2], fy * RS1[1] + cy * RS1[2], fy * mc[1] + cy * mc[2]};
+    const double M2[3] = {RS0[2], RS1[2], mc[2]};
+    const double distance = M2[0] * M2[0] + M2[1] * M2[1] - M2[2] * M2[2];
+    if (distance == 0.0) return false;
+    const double f = 1.0 / distance;
+    const double mx = f * (M0[0] * M2[0] + M0[1] * M2[1] - M0[2] * M2[2]);
+    const double my = f * (M1[0] * M2[0] + M1[1] * M2[1] - M1[2] * M2[2]);
+    const double tx = f * (M0[0] * M0[0] + M0[1] * M0[1] - M0[2] * M0[2]);
+    const double ty = f * (M1[0] * M1[0] + M1[1] * M1[1] - M1[2] * M1[2]);
+    const double radius = ceil(3.0 * sqrt(fmax(1e-4, fmax(mx * mx - tx, my * my - ty))));
+    if (!(radius > (double)radius_clip)) return false;
+    if (mx + radius <= 0.0 || mx - radius >= (double)width || my + radius <= 0.0 || my - radius >= (double)height)
+        return false;
+    const double mult = -(RS2[0] * mc[0] + RS2[1] * mc[1] + RS2[2] * mc[2]) > 0.0 ? 1.0 : -1.0;
+    o.radius = (int32_t)fmin(radius, 2147483647.0);  // saturates as the FP32 path's conversion does
+    o.m2d = make_float2((float)mx, (float)my);
+    o.depth = (float)mc[2];
+    for (int k = 0; k < 3; ++k) {
+        o.M[k] = (float)M0[k];
+        o.M[3 + k] = (float)M1[k];
+        o.M[6 + k] = (float)M2[k];
+    }
+    o.nrm = mk3((float)(mult * RS2[0]), (float)(mult * RS2[1]), (float)(mult * RS2[2]));
+    return true;
+}
+
+// Below this |distance| / |M2|^2 the FP32 solve has lost 6 or more of its 24
+// bits to cancellation (the splat's plane passes close to the camera centre:
+// relative error of means2d ~1e-8 / ratio), and the projection is redone in
+// FP64.  Ordinary splats (scale << depth) have a ratio near 1 and never
+// take this path.
+constexpr float kDegenerateRel = 1.0f / 64.0f;
 
 // Projects Gaussian n into camera c; false when it is culled (near/far plane,
 // degenerate transform, radius clip or off-screen box).
@@ -58,7 +127,9 @@ __device__ __forceinline__ bool project_one(const float* __restrict__ means, con
     const f3 M1 = mk3(fy * RS0.y + cy * RS0.z, fy * RS1.y + cy * RS1.z, fy * mc.y + cy * mc.z);
     const f3 M2 = mk3(RS0.z, RS1.z, mc.z);
     const float distance = M2.x * M2.x + M2.y * M2.y - M2.z * M2.z;
-    if (distance == 0.f) return false;
+    if (fabsf(distance) < kDegenerateRel * (M2.x * M2.x + M2.y * M2.y + M2.z * M2.z))
+        return project_one_f64(means, quats, scales, viewmats, Ks, width, height, near_plane, far_plane, radius_clip,
+                               c, n, o);
     const float inv = 1.f / distance;
     const f3 f = mk3(inv, inv, -inv);
     const float mx = f.x * M0.x * M2.x + f.y * M0.y * M2.y + f.z * M0.z * M2.z;
@@ -94,6 +165,57 @@ __device__ __forceinline__ void store_projected(const Projected& o, int64_t i, i
     normals[3 * i + 2] = o.nrm.z;
 }
 
+// Camera centre of a world-to-camera matrix [R | t]: -R^-1 t, the translation
+// of the inverse view matrix (R^-1 by cofactors, so R need not be orthonormal).
+__device__ __forceinline__ f3 camera_centre(const float* __restrict__ vm) {
+    const float a = vm[0], b = vm[1], c = vm[2], d = vm[4], e = vm[5], f = vm[6], g = vm[8], h = vm[9], i = vm[10];
+    const float c00 = e * i - f * h, c01 = f * g - d * i, c02 = d * h - e * g;
+    const float c10 = c * h - b * i, c11 = a * i - c * g, c12 = b * g - a * h;
+    const float c20 = b * f - c * e, c21 = c * d - a * f, c22 = a * e - b * d;
+    const float inv_det = 1.f / (a * c00 + b * c01 + c * c02);
+    const float t0 = vm[3], t1 = vm[7], t2 = vm[11];
+    return mk3(-(c00 * t0 + c10 * t1 + c20 * t2) * inv_det, -(c01 * t0 + c11 * t1 + c21 * t2) * inv_det,
+               -(c02 * t0 + c12 * t1 + c22 * t2) * inv_det);
+}
+
+// Fused SH colour of Gaussian n seen from camera c: max(SH + 0.5, 0) for a
+// visible entry, 0.5 (the value the unfused path gives a masked entry) otherwise.
+__device__ __forceinline__ f3 fused_sh_color(const float* __restrict__ means, const float* __restrict__ viewmats,
+                                             int degree, int K, const float* __restrict__ coeffs, int c, int64_t n,
+                                             bool visible) {
+    if (!visible) return mk3(0.5f, 0.5f, 0.5f);
+    const f3 o = camera_centre(viewmats + 16 * c);
+    const f3 d = mk3(means[3 * n] - o.x, means[3 * n + 1] - o.y, means[3 * n + 2] - o.z);
+    const f3 col = sh_color(degree, d, coeffs + n * K * 3);
+    return mk3(fmaxf(col.x + 0.5f, 0.f), fmaxf(col.y + 0.5f, 0.f), fmaxf(col.z + 0.5f, 0.f));
+}
+
+__device__ __forceinline__ void store3(float* dst, int64_t i, f3 v) {
+    dst[3 * i] = v.x;
+    dst[3 * i + 1] = v.y;
+    dst[3 * i + 2] = v.z;
+}
+
+// Adjoint of fused_sh_color for a visible entry with NB = (degree+1)^2 bases:
+// the clamp passes the gradient where SH + 0.5 >= 0 (as torch.clamp_min's
+// backward does); coefficient gradients are added into acc[3*NB], the
+// direction gradient is returned (it is the gradient of the mean, the camera
+// centre being a constant).
+template <int NB>
+__device__ __forceinline__ f3 fused_sh_vjp(const float* __restrict__ means, const float* __restrict__ viewmats,
+                                           int K, const float* __restrict__ coeffs, int c, int64_t n, f3 g,
+                                           float* acc) {
+    constexpr int degree = NB == 1 ? 0 : NB == 4 ? 1 : NB == 9 ? 2 : NB == 16 ? 3 : 4;
+    const f3 o = camera_centre(viewmats + 16 * c);
+    const f3 d = mk3(means[3 * n] - o.x, means[3 * n + 1] - o.y, means[3 * n + 2] - o.z);
+    const float* crow = coeffs + n * K * 3;
+    const f3 col = sh_color(degree, d, crow);
+    g.x = col.x + 0.5f >= 0.f ? g.x : 0.f;
+    g.y = col.y + 0.5f >= 0.f ? g.y : 0.f;
+    g.z = col.z + 0.5f >= 0.f ? g.z : 0.f;
+    return sh_color_vjp<NB>(degree, d, crow, g, acc);
+}
+
 __global__ void __launch_bounds__(256) project_fwd_kernel(tg_project_fwd_args a) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t total = (int64_t)a.C * a.N;
@@ -101,8 +223,9 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(tg_project_fwd_args a)
     const int c = (int)(idx / a.N);
     const int64_t n = idx - (int64_t)c * a.N;
     Projected o;
-    if (!project_one(a.means, a.quats, a.scales, a.viewmats, a.Ks, a.width, a.height, a.near_plane, a.far_plane,
-                     a.radius_clip, c, n, o)) {
+    const bool vis = project_one(a.means, a.quats, a.scales, a.viewmats, a.Ks, a.width, a.height, a.near_plane,
+                                 a.far_plane, a.radius_clip, c, n, o);
+    if (!vis) {
         o.radius = 0;
         o.m2d = make_float2(0.f, 0.f);
         o.depth = 0.f;
@@ -111,6 +234,8 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(tg_project_fwd_args a)
         o.nrm = mk3(0, 0, 0);
     }
     store_projected(o, idx, a.radii, a.means2d, a.depths, a.ray_transforms, a.normals);
+    if (a.sh_coeffs)
+        store3(a.colors, idx, fused_sh_color(a.means, a.viewmats, a.sh_degree, a.sh_K, a.sh_coeffs, c, n, vis));
 }
 
 // ------------------------------------------------------------------ packed forward
@@ -206,6 +331,9 @@ __global__ void __launch_bounds__(kPackThreads) project_packed_emit_kernel(tg_pr
                 a.camera_ids[pos] = c;
                 a.gaussian_ids[pos] = n;
                 store_projected(o, pos, a.radii, a.means2d, a.depths, a.ray_transforms, a.normals);
+                if (a.sh_coeffs)
+                    store3(a.colors, pos,
+                           fused_sh_color(a.means, a.viewmats, a.sh_degree, a.sh_K, a.sh_coeffs, c, n, true));
             } else if (a.overflow) {
                 atomicOr(a.overflow, 1u);
             }
@@ -323,9 +451,18 @@ __device__ __forceinline__ EntryGrad project_entry_vjp(const float* __restrict__
     return out;
 }
 
+// NB: SH bases of the fused SH adjoint ((degree+1)^2; 0 = no fused SH), which
+// sizes the per-thread coefficient-gradient accumulator.
+template <int NB>
 __global__ void __launch_bounds__(256) project_bwd_kernel(tg_project_bwd_args a) {
+    constexpr bool kSH = NB > 0;
     const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= a.N) return;
+    float acc[kSH ? 3 * NB : 1];  // SH coefficient gradient, summed over cameras in registers
+    if constexpr (kSH) {
+#pragma unroll
+        for (int k = 0; k < 3 * NB; ++k) acc[k] = 0.f;
+    }
     const f3 p = mk3(a.means[3 * n], a.means[3 * n + 1], a.means[3 * n + 2]);
     const float4 q = __ldg(reinterpret_cast<const float4*>(a.quats) + n);
     const float s0 = a.scales[3 * n], s1 = a.scales[3 * n + 1];
@@ -344,6 +481,16 @@ __global__ void __launch_bounds__(256) project_bwd_kernel(tg_project_bwd_args a)
         v_s0 += g.v_s0;
         v_s1 += g.v_s1;
         v_mean = v_mean + g.v_mean;
+        if constexpr (kSH) {
+            const f3 gc = mk3(a.v_colors[3 * idx], a.v_colors[3 * idx + 1], a.v_colors[3 * idx + 2]);
+            v_mean = v_mean + fused_sh_vjp<NB>(a.means, a.viewmats, a.sh_K, a.sh_coeffs, c, n, gc, acc);
+        }
+    }
+    if constexpr (kSH) {
+        float* vc = a.v_sh_coeffs + n * a.sh_K * 3;
+#pragma unroll
+        for (int k = 0; k < 3 * NB; ++k) vc[k] = acc[k];
+        for (int k = 3 * NB; k < 3 * a.sh_K; ++k) vc[k] = 0.f;
     }
     a.v_means[3 * n] = v_mean.x;
     a.v_means[3 * n + 1] = v_mean.y;
@@ -358,11 +505,27 @@ __global__ void __launch_bounds__(256) project_bwd_kernel(tg_project_bwd_args a)
 // written at its own row.  Dense: added into the Gaussian's row with float
 // atomics (entries of one Gaussian sit C-strided apart in camera-major order,
 // so there is nothing to combine inside a warp first).
+template <int NB>
 __global__ void __launch_bounds__(256) project_packed_bwd_kernel(tg_project_packed_bwd_args a) {
+    constexpr bool kSH = NB > 0;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nnz) return;
     const int64_t c = a.camera_ids[i], n = a.gaussian_ids[i];
     if (c < 0 || c >= a.C || n < 0 || n >= a.N) return;
+    f3 v_dir = mk3(0, 0, 0);
+    if constexpr (kSH) {
+        float acc[3 * NB];
+#pragma unroll
+        for (int k = 0; k < 3 * NB; ++k) acc[k] = 0.f;
+        const f3 gc = mk3(a.v_colors[3 * i], a.v_colors[3 * i + 1], a.v_colors[3 * i + 2]);
+        if (gc.x != 0.f || gc.y != 0.f || gc.z != 0.f) {
+            v_dir = fused_sh_vjp<NB>(a.means, a.viewmats, a.sh_K, a.sh_coeffs, (int)c, n, gc, acc);
+            float* vc = a.v_sh_coeffs + n * a.sh_K * 3;
+#pragma unroll
+            for (int k = 0; k < 3 * NB; ++k)
+                if (acc[k] != 0.f) atomicAdd(vc + k, acc[k]);
+        }
+    }
     const f3 p = mk3(a.means[3 * n], a.means[3 * n + 1], a.means[3 * n + 2]);
     const float4 q = __ldg(reinterpret_cast<const float4*>(a.quats) + n);
     const float s0 = a.scales[3 * n], s1 = a.scales[3 * n + 1];
@@ -371,18 +534,19 @@ __global__ void __launch_bounds__(256) project_packed_bwd_kernel(tg_project_pack
         a.viewmats, a.Ks, (int)c, p, q, s0, s1, Rq, a.ray_transforms + 9 * i, a.v_ray_transforms + 9 * i,
         a.v_depths[i], a.v_means2d[2 * i], a.v_means2d[2 * i + 1],
         mk3(a.v_normals[3 * i], a.v_normals[3 * i + 1], a.v_normals[3 * i + 2]), a.mode);
+    const f3 vm_total = g.v_mean + v_dir;
     if (a.sparse_grad) {
-        a.v_means[3 * i] = g.v_mean.x;
-        a.v_means[3 * i + 1] = g.v_mean.y;
-        a.v_means[3 * i + 2] = g.v_mean.z;
+        a.v_means[3 * i] = vm_total.x;
+        a.v_means[3 * i + 1] = vm_total.y;
+        a.v_means[3 * i + 2] = vm_total.z;
         reinterpret_cast<float4*>(a.v_quats)[i] = g.v_quat;
         a.v_scales[3 * i] = g.v_s0;
         a.v_scales[3 * i + 1] = g.v_s1;
         a.v_scales[3 * i + 2] = 0.f;
     } else {
-        atomicAdd(a.v_means + 3 * n, g.v_mean.x);
-        atomicAdd(a.v_means + 3 * n + 1, g.v_mean.y);
-        atomicAdd(a.v_means + 3 * n + 2, g.v_mean.z);
+        atomicAdd(a.v_means + 3 * n, vm_total.x);
+        atomicAdd(a.v_means + 3 * n + 1, vm_total.y);
+        atomicAdd(a.v_means + 3 * n + 2, vm_total.z);
         atomicAdd(reinterpret_cast<float4*>(a.v_quats) + n, g.v_quat);
         atomicAdd(a.v_scales + 3 * n, g.v_s0);
         atomicAdd(a.v_scales + 3 * n + 1, g.v_s1);
@@ -399,7 +563,15 @@ cudaError_t launch_project_fwd(const tg_project_fwd_args& a, cudaStream_t s) {
 
 cudaError_t launch_project_bwd(const tg_project_bwd_args& a, cudaStream_t s) {
     if (a.N == 0) return cudaSuccess;
-    project_bwd_kernel<<<(unsigned)((a.N + 255) / 256), 256, 0, s>>>(a);
+    const unsigned grid = (unsigned)((a.N + 255) / 256);
+    switch (a.sh_coeffs ? a.sh_degree : -1) {
+        case 0: project_bwd_kernel<1><<<grid, 256, 0, s>>>(a); break;
+        case 1: project_bwd_kernel<4><<<grid, 256, 0, s>>>(a); break;
+        case 2: project_bwd_kernel<9><<<grid, 256, 0, s>>>(a); break;
+        case 3: project_bwd_kernel<16><<<grid, 256, 0, s>>>(a); break;
+        case 4: project_bwd_kernel<25><<<grid, 256, 0, s>>>(a); break;
+        default: project_bwd_kernel<0><<<grid, 256, 0, s>>>(a); break;
+    }
     note_launches(1);
     return cudaGetLastError();
 }
@@ -452,7 +624,15 @@ cudaError_t launch_project_packed_emit(const tg_project_packed_args& a, cudaStre
 
 cudaError_t launch_project_packed_bwd(const tg_project_packed_bwd_args& a, cudaStream_t s) {
     if (a.nnz == 0) return cudaSuccess;
-    project_packed_bwd_kernel<<<(unsigned)((a.nnz + 255) / 256), 256, 0, s>>>(a);
+    const unsigned grid = (unsigned)((a.nnz + 255) / 256);
+    switch (a.sh_coeffs ? a.sh_degree : -1) {
+        case 0: project_packed_bwd_kernel<1><<<grid, 256, 0, s>>>(a); break;
+        case 1: project_packed_bwd_kernel<4><<<grid, 256, 0, s>>>(a); break;
+        case 2: project_packed_bwd_kernel<9><<<grid, 256, 0, s>>>(a); break;
+        case 3: project_packed_bwd_kernel<16><<<grid, 256, 0, s>>>(a); break;
+        case 4: project_packed_bwd_kernel<25><<<grid, 256, 0, s>>>(a); break;
+        default: project_packed_bwd_kernel<0><<<grid, 256, 0, s>>>(a); break;
+    }
     note_launches(1);
     return cudaGetLastError();
 }

@@ -1,64 +1,11 @@
 // Spherical-harmonics colour evaluation (degree <= 4) and its adjoint, sm_100a.
 //
-// Bases follow the real-SH convention of the reference
-// (textured_gaussians/cuda/csrc/spherical_harmonics.cuh:17-111, which uses
-// Sloan, "Efficient Spherical Harmonic Evaluation", JCGT 2013).  The adjoint
-// w.r.t. the direction is taken with forward-mode dual numbers over the same
-// basis code, so no hand-derived derivative table is needed.  One thread per
-// (camera, Gaussian) element computes all three channels.
-#include "tg_common.cuh"
+// Bases and their dual-number adjoint are in sh_eval.cuh (the reference's
+// convention, textured_gaussians/cuda/csrc/spherical_harmonics.cuh:17-111).
+// One thread per (camera, Gaussian) element computes all three channels.
+#include "sh_eval.cuh"
 
 namespace tg {
-
-struct Dual {
-    float v, d0, d1, d2;
-};
-__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d0 + b.d0, a.d1 + b.d1, a.d2 + b.d2}; }
-__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d0 - b.d0, a.d1 - b.d1, a.d2 - b.d2}; }
-__device__ __forceinline__ Dual operator*(Dual a, Dual b) {
-    return {a.v * b.v, a.d0 * b.v + a.v * b.d0, a.d1 * b.v + a.v * b.d1, a.d2 * b.v + a.v * b.d2};
-}
-__device__ __forceinline__ Dual operator*(float s, Dual a) { return {s * a.v, s * a.d0, s * a.d1, s * a.d2}; }
-__device__ __forceinline__ Dual operator+(Dual a, float s) { return {a.v + s, a.d0, a.d1, a.d2}; }
-
-template <typename S>
-__device__ __forceinline__ void sh_bases(int degree, S x, S y, S z, S* b) {
-    b[0] = S{} + 0.2820947917738781f;
-    if (degree < 1) return;
-    b[1] = -0.48860251190292f * y;
-    b[2] = 0.48860251190292f * z;
-    b[3] = -0.48860251190292f * x;
-    if (degree < 2) return;
-    const S z2 = z * z, fC1 = x * x - y * y, fS1 = 2.f * (x * y);
-    b[4] = 0.5462742152960395f * fS1;
-    b[5] = -1.092548430592079f * (z * y);
-    b[6] = 0.9461746957575601f * z2 + (-0.3153915652525201f);
-    b[7] = -1.092548430592079f * (z * x);
-    b[8] = 0.5462742152960395f * fC1;
-    if (degree < 3) return;
-    const S fC2 = x * fC1 - y * fS1, fS2 = x * fS1 + y * fC1;
-    const S t0c = -2.285228997322329f * z2 + 0.4570457994644658f;
-    b[9] = -0.5900435899266435f * fS2;
-    b[10] = 1.445305721320277f * (z * fS1);
-    b[11] = t0c * y;
-    b[12] = z * (1.865881662950577f * z2 + (-1.119528997770346f));
-    b[13] = t0c * x;
-    b[14] = 1.445305721320277f * (z * fC1);
-    b[15] = -0.5900435899266435f * fC2;
-    if (degree < 4) return;
-    const S fC3 = x * fC2 - y * fS2, fS3 = x * fS2 + y * fC2;
-    const S t0d = z * (-4.683325804901025f * z2 + 2.007139630671868f);
-    const S t1c = 3.31161143515146f * z2 + (-0.47308734787878f);
-    b[16] = 0.6258357354491763f * fS3;
-    b[17] = -1.770130769779931f * (z * fS2);
-    b[18] = t1c * fS1;
-    b[19] = t0d * y;
-    b[20] = 1.984313483298443f * (z * b[12]) - 1.006230589874905f * b[6];
-    b[21] = t0d * x;
-    b[22] = t1c * fC1;
-    b[23] = -1.770130769779931f * (z * fC2);
-    b[24] = 0.6258357354491763f * fC3;
-}
 
 __global__ void sh_fwd_kernel(int64_t n, int64_t rows, int degree, int K, const float* __restrict__ dirs,
                               const float* __restrict__ coeffs, const uint8_t* __restrict__ masks,

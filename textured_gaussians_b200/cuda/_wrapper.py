@@ -138,6 +138,8 @@ def fully_fused_projection_2dgs(
     norm_rot_grad: bool = False,
     *,
     adjoint: str = "reference",
+    sh_coeffs: Optional[Tensor] = None,
+    sh_degree: Optional[int] = None,
 ) -> Tuple[Tensor, ...]:
     """Ray-splat transforms, 2D means, depths, screen radii and normals
     (reference: cuda/_wrapper.py:1267-1371).
@@ -151,6 +153,12 @@ def fully_fused_projection_2dgs(
     ``adjoint="exact"`` selects the exact derivative of means2d with respect
     to the ray transform in the backward (the reference keeps only its
     diagonal terms).
+
+    ``sh_coeffs`` [N,K,3] with ``sh_degree`` fuses the renderer's SH colour
+    step into the projection (reference glue: rendering.py:1573-1583): one
+    more output, the colours ``max(SH(degree, mean - camera centre) + 0.5, 0)``
+    per visible entry ([C,N,3] or [nnz,3]; 0.5 for culled entries), whose
+    adjoint reaches ``sh_coeffs`` and ``means``.
     """
     C = viewmats.size(0)
     N = means.size(0)
@@ -164,13 +172,18 @@ def fully_fused_projection_2dgs(
     if sparse_grad:
         assert packed, "sparse_grad is only supported when packed is True"
     mode = B.TG_ADJ_EXACT if adjoint == "exact" else (B.TG_ADJ_BWD2 if norm_rot_grad else B.TG_ADJ_REFERENCE)
+    if sh_coeffs is not None:
+        assert sh_degree is not None and sh_coeffs.dim() == 3 and sh_coeffs.shape[0] == N, sh_coeffs.shape
+        assert sh_coeffs.shape[2] == 3 and (sh_degree + 1) ** 2 <= sh_coeffs.shape[1] <= 25, sh_coeffs.shape
+        sh_coeffs = sh_coeffs.float().contiguous()
+    sh = (sh_coeffs, int(sh_degree or 0))
     if packed:
         return _FullyFusedProjectionPacked2DGS.apply(
             means.contiguous(), quats.contiguous(), scales.contiguous(), viewmats.contiguous(), Ks.contiguous(),
-            width, height, eps2d, near_plane, far_plane, radius_clip, sparse_grad, mode, None)
+            width, height, eps2d, near_plane, far_plane, radius_clip, sparse_grad, mode, None, *sh)
     return _FullyFusedProjection2DGS.apply(
         means.contiguous(), quats.contiguous(), scales.contiguous(), viewmats.contiguous(), Ks.contiguous(),
-        width, height, eps2d, near_plane, far_plane, radius_clip, mode)
+        width, height, eps2d, near_plane, far_plane, radius_clip, mode, *sh)
 
 
 class _FullyFusedProjection2DGS(torch.autograd.Function):
@@ -178,7 +191,7 @@ class _FullyFusedProjection2DGS(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, means, quats, scales, viewmats, Ks, width, height, eps2d, near_plane, far_plane, radius_clip,
-                mode):
+                mode, sh_coeffs=None, sh_degree=0):
         C, N = viewmats.shape[0], means.shape[0]
         dev = means.device
         radii = torch.empty((C, N), dtype=torch.int32, device=dev)
@@ -189,17 +202,24 @@ class _FullyFusedProjection2DGS(torch.autograd.Function):
         a = B.ProjectFwdArgs(C, N, B.ptr(means), B.ptr(quats), B.ptr(scales), B.ptr(viewmats), B.ptr(Ks),
                              int(width), int(height), float(near_plane), float(far_plane), float(radius_clip),
                              B.ptr(radii), B.ptr(means2d), B.ptr(depths), B.ptr(ray_transforms), B.ptr(normals))
+        colors = None
+        if sh_coeffs is not None:
+            colors = torch.empty((C, N, 3), dtype=torch.float32, device=dev)
+            a.sh_degree, a.sh_K, a.sh_coeffs, a.colors = sh_degree, sh_coeffs.shape[1], B.ptr(sh_coeffs), B.ptr(colors)
         if C * N:
             st = B.stream_of(means)
             B.call("tg_project_fwd", st, B.lib().tg_project_fwd, ctypes.byref(a), st)
-        ctx.save_for_backward(means, quats, scales, viewmats, Ks, radii, ray_transforms)
+        ctx.save_for_backward(means, quats, scales, viewmats, Ks, radii, ray_transforms, sh_coeffs)
         ctx.mode = mode
+        ctx.sh_degree = sh_degree
         ctx.mark_non_differentiable(radii)
+        if colors is not None:
+            return radii, means2d, depths, ray_transforms, normals, colors
         return radii, means2d, depths, ray_transforms, normals
 
     @staticmethod
-    def backward(ctx, v_radii, v_means2d, v_depths, v_ray_transforms, v_normals):
-        means, quats, scales, viewmats, Ks, radii, ray_transforms = ctx.saved_tensors
+    def backward(ctx, v_radii, v_means2d, v_depths, v_ray_transforms, v_normals, v_colors=None):
+        means, quats, scales, viewmats, Ks, radii, ray_transforms, sh_coeffs = ctx.saved_tensors
         C, N = viewmats.shape[0], means.shape[0]
 
         def z(t, shape):
@@ -216,13 +236,19 @@ class _FullyFusedProjection2DGS(torch.autograd.Function):
                              B.ptr(radii), B.ptr(ray_transforms), B.ptr(v_means2d), B.ptr(v_depths),
                              B.ptr(v_normals), B.ptr(v_ray_transforms), ctx.mode, B.ptr(v_means), B.ptr(v_quats),
                              B.ptr(v_scales))
+        v_sh = None
+        if sh_coeffs is not None:
+            v_col = z(v_colors, (C, N, 3))
+            v_sh = torch.empty_like(sh_coeffs)
+            a.sh_degree, a.sh_K, a.sh_coeffs = ctx.sh_degree, sh_coeffs.shape[1], B.ptr(sh_coeffs)
+            a.v_colors, a.v_sh_coeffs = B.ptr(v_col), B.ptr(v_sh)
         if N:
             st = B.stream_of(means)
             B.call("tg_project_bwd", st, B.lib().tg_project_bwd, ctypes.byref(a), st)
         v_viewmats = torch.zeros_like(viewmats) if ctx.needs_input_grad[3] else None  # never written (reference)
         return (v_means if ctx.needs_input_grad[0] else None, v_quats if ctx.needs_input_grad[1] else None,
                 v_scales if ctx.needs_input_grad[2] else None, v_viewmats,
-                None, None, None, None, None, None, None, None)
+                None, None, None, None, None, None, None, None, v_sh, None)
 
 
 class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
@@ -235,7 +261,7 @@ class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, means, quats, scales, viewmats, Ks, width, height, eps2d, near_plane, far_plane, radius_clip,
-                sparse_grad, mode, batch):
+                sparse_grad, mode, batch, sh_coeffs=None, sh_degree=0):
         C, N = viewmats.shape[0], means.shape[0]
         dev = means.device
         ws = torch.empty((B.lib().tg_project_packed_workspace_bytes(C, N),), dtype=torch.uint8, device=dev)
@@ -267,16 +293,24 @@ class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
         a.camera_ids, a.gaussian_ids, a.radii = B.ptr(camera_ids), B.ptr(gaussian_ids), B.ptr(radii)
         a.means2d, a.depths, a.ray_transforms, a.normals = (B.ptr(means2d), B.ptr(depths), B.ptr(ray_transforms),
                                                             B.ptr(normals))
+        colors = None
+        if sh_coeffs is not None:
+            colors = torch.empty((nnz, 3), dtype=torch.float32, device=dev)
+            a.sh_degree, a.sh_K, a.sh_coeffs, a.colors = sh_degree, sh_coeffs.shape[1], B.ptr(sh_coeffs), B.ptr(colors)
         B.call("tg_project_packed_emit", st, B.lib().tg_project_packed_emit, ctypes.byref(a), st)
-        ctx.save_for_backward(camera_ids, gaussian_ids, means, quats, scales, viewmats, Ks, ray_transforms)
+        ctx.save_for_backward(camera_ids, gaussian_ids, means, quats, scales, viewmats, Ks, ray_transforms, sh_coeffs)
         ctx.sparse_grad = bool(sparse_grad)
         ctx.mode = mode
+        ctx.sh_degree = sh_degree
         ctx.mark_non_differentiable(camera_ids, gaussian_ids, radii)
+        if colors is not None:
+            return camera_ids, gaussian_ids, radii, means2d, depths, ray_transforms, normals, colors
         return camera_ids, gaussian_ids, radii, means2d, depths, ray_transforms, normals
 
     @staticmethod
-    def backward(ctx, v_camera_ids, v_gaussian_ids, v_radii, v_means2d, v_depths, v_ray_transforms, v_normals):
-        camera_ids, gaussian_ids, means, quats, scales, viewmats, Ks, ray_transforms = ctx.saved_tensors
+    def backward(ctx, v_camera_ids, v_gaussian_ids, v_radii, v_means2d, v_depths, v_ray_transforms, v_normals,
+                 v_colors=None):
+        camera_ids, gaussian_ids, means, quats, scales, viewmats, Ks, ray_transforms, sh_coeffs = ctx.saved_tensors
         C, N, nnz = viewmats.shape[0], means.shape[0], camera_ids.shape[0]
         dev = means.device
 
@@ -295,6 +329,12 @@ class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
                                    B.ptr(camera_ids), B.ptr(gaussian_ids), B.ptr(ray_transforms), B.ptr(v_means2d),
                                    B.ptr(v_depths), B.ptr(v_normals), B.ptr(v_ray_transforms), ctx.mode,
                                    int(ctx.sparse_grad), B.ptr(v_means), B.ptr(v_quats), B.ptr(v_scales))
+        v_sh = None
+        if sh_coeffs is not None:
+            v_col = z(v_colors, (nnz, 3))
+            v_sh = torch.empty_like(sh_coeffs)
+            a.sh_degree, a.sh_K, a.sh_coeffs = ctx.sh_degree, sh_coeffs.shape[1], B.ptr(sh_coeffs)
+            a.v_colors, a.v_sh_coeffs = B.ptr(v_col), B.ptr(v_sh)
         st = B.stream_of(means)
         B.call("tg_project_packed_bwd", st, B.lib().tg_project_packed_bwd, ctypes.byref(a), st)
 
@@ -310,7 +350,7 @@ class _FullyFusedProjectionPacked2DGS(torch.autograd.Function):
         v_viewmats = torch.zeros_like(viewmats) if ctx.needs_input_grad[4] else None
         return (out(v_means, means, ctx.needs_input_grad[0]), out(v_quats, quats, ctx.needs_input_grad[1]),
                 out(v_scales, scales, ctx.needs_input_grad[2]), v_viewmats,
-                None, None, None, None, None, None, None, None, None, None)
+                None, None, None, None, None, None, None, None, None, None, v_sh, None)
 
 
 # --------------------------------------------------------------------------- intersection

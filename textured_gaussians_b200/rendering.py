@@ -19,8 +19,10 @@ adjoint end to end), ``tile_order`` ("heaviest_first", the default: compositor
 tiles taken by descending intersection count, so the longest tiles do not form
 the launch's tail; "launch": tile index order; the results are the same),
 ``batch_depth`` (splats staged per compositor batch; 0 = tile_size^2),
-``persistent`` (compositor CTAs take tiles from a device work counter) and
-``tile_size`` 32 besides the reference's 8 and 16.
+``persistent`` (compositor CTAs take tiles from a device work counter),
+``tile_size`` 32 besides the reference's 8 and 16, and ``fuse_sh`` (default
+on: the SH colours are computed inside the projection kernels instead of the
+reference's separate SH op + camera-centre inverse + clamp glue).
 """
 from __future__ import annotations
 
@@ -54,7 +56,7 @@ def _inverse(m: Tensor) -> Tensor:
 
 def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, height, near_plane, far_plane,
              radius_clip, eps2d, sh_degree, packed, tile_size, render_mode, sparse_grad, norm_rot_grad, distloss,
-             adjoint, tile_order="heaviest_first"):
+             adjoint, tile_order="heaviest_first", fuse_sh=True):
     assert tile_order in ("launch", "heaviest_first"), tile_order
     N = means.shape[0]
     C = viewmats.shape[0]
@@ -75,14 +77,16 @@ def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, heigh
         assert colors.dim() == 3 and colors.shape[0] == N and colors.shape[2] == 3, colors.shape
         assert (sh_degree + 1) ** 2 <= colors.shape[1], colors.shape
 
+    fuse = fuse_sh and sh_degree is not None
     proj = fully_fused_projection_2dgs(
         means, quats, scales, viewmats, Ks, width, height, eps2d, near_plane, far_plane, radius_clip, packed,
-        sparse_grad, norm_rot_grad, adjoint=adjoint)
+        sparse_grad, norm_rot_grad, adjoint=adjoint, sh_coeffs=colors if fuse else None,
+        sh_degree=sh_degree if fuse else None)
     if packed:
-        camera_ids, gaussian_ids, radii, means2d, depths, ray_transforms, normals = proj
+        camera_ids, gaussian_ids, radii, means2d, depths, ray_transforms, normals = proj[:7]
         opacities = opacities[gaussian_ids]
     else:
-        radii, means2d, depths, ray_transforms, normals = proj
+        radii, means2d, depths, ray_transforms, normals = proj[:5]
         opacities = opacities.repeat(C, 1)
         camera_ids, gaussian_ids = None, None
 
@@ -96,7 +100,9 @@ def _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, heigh
     order = (tile_order_heaviest_first(isect_offsets, n_isects_of(flatten_ids)) if tile_order == "heaviest_first"
              else None)
 
-    if sh_degree is not None:
+    if fuse:
+        colors = proj[-1]  # SH colours computed inside the projection, +0.5 and clamp applied
+    elif sh_degree is not None:
         camtoworlds = _inverse(viewmats)
         if packed:
             dirs = means[gaussian_ids, :] - camtoworlds[camera_ids, :3, 3]
@@ -187,6 +193,7 @@ def rasterization_2dgs(
     tile_order: str = "heaviest_first",
     batch_depth: int = 0,
     persistent: bool = False,
+    fuse_sh: bool = True,
 ) -> Tuple[Tensor, Tensor, Tensor, Optional[Tensor], Tensor, Tensor, Tensor, Tensor, Dict]:
     """Rasterize 2D Gaussian surfels (N) to C image planes (reference: rendering.py:1009-1338).
 
@@ -196,7 +203,7 @@ def rasterization_2dgs(
     """
     p = _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, height, near_plane, far_plane,
                  radius_clip, eps2d, sh_degree, packed, tile_size, render_mode, sparse_grad, norm_rot_grad, distloss,
-                 adjoint, tile_order)
+                 adjoint, tile_order, fuse_sh)
     outs = rasterize_to_pixels_2dgs(
         p["means2d"], p["ray_transforms"], p["colors"], p["opacities"], p["normals"], p["densify"], width, height,
         tile_size, p["isect_offsets"], p["flatten_ids"], backgrounds=backgrounds, packed=packed, absgrad=absgrad,
@@ -243,6 +250,7 @@ def rasterization_textured_gaussians(
     tile_order: str = "heaviest_first",
     batch_depth: int = 0,
     persistent: bool = False,
+    fuse_sh: bool = True,
 ) -> Tuple[Tensor, Tensor, Tensor, Optional[Tensor], Tensor, Tensor, Tensor, Tensor, Dict]:
     """Rasterize textured 2D Gaussian surfels (reference: rendering.py:1342-1685).
 
@@ -254,7 +262,7 @@ def rasterization_textured_gaussians(
     assert textures.shape[0] == N and textures.shape[-1] == 4 and textures.dim() == 4, textures.shape
     p = _prepare(means, quats, scales, opacities, colors, viewmats, Ks, width, height, near_plane, far_plane,
                  radius_clip, eps2d, sh_degree, packed, tile_size, render_mode, sparse_grad, norm_rot_grad, distloss,
-                 adjoint, tile_order)
+                 adjoint, tile_order, fuse_sh)
     outs = rasterize_to_pixels_textured_gaussians(
         p["means2d"], p["ray_transforms"], p["colors"], p["opacities"], textures, texture_range_x, texture_range_y,
         p["normals"], p["densify"], width, height, tile_size, p["isect_offsets"], p["flatten_ids"],
