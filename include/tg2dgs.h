@@ -417,6 +417,40 @@ TG_API int tg_sh_fwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, c
 TG_API int tg_sh_bwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, const float* dirs, const float* coeffs,
                      const uint8_t* masks, const float* v_colors, float* v_coeffs, float* v_dirs, tg_stream_t stream);
 
+/* ------------------------------------------------------------------ gradient consumers
+ * Replaces selective_adam_update (textured_gaussians/cuda/csrc/adam.cu:17-89):
+ * for every row r < N (M floats each) with visibility[r] != 0,
+ *   m = b1 m + (1-b1) g;  v = b2 v + (1-b2) g^2;  p += -lr m / (sqrt(v) + eps)
+ * (no bias correction, as in the reference); other rows are not touched.
+ * shadow_format TG_TEX_BF16 / TG_TEX_F16 additionally writes each updated
+ * row into `shadow` ([N*M] in that format: the texture storage the compositor
+ * samples) in the same pass; TG_TEX_NONE: no shadow. */
+TG_API int tg_selective_adam(float* param, const float* grad, float* exp_avg, float* exp_avg_sq,
+                             const uint8_t* visibility, float lr, float b1, float b2, float eps, int64_t N, int64_t M,
+                             int32_t shadow_format, void* shadow, tg_stream_t stream);
+
+/* Replaces the running-statistics update of DefaultStrategy._update_state
+ * (textured_gaussians/strategy/default.py:213-261): for every entry with
+ * radius > 0, grad2d[g] += |(gx * width/2 * C, gy * height/2 * C)|,
+ * count[g] += 1 and (if max_radii != NULL) max_radii[g] = max(max_radii[g],
+ * radius / max(width, height)) -- a true maximum (the reference's indexed
+ * assignment keeps the last camera's value when a Gaussian is seen by several).
+ * Dense: entries [C,N], g = n; packed: gaussian_ids[e].  max_radii must hold
+ * non-negative values. */
+typedef struct {
+    int32_t C;
+    int64_t N;                  /* Gaussians */
+    int64_t n_elems;            /* packed: nnz (dense: C*N, unused) */
+    const float* grads2d;       /* [E,2] gradient of the 2D means (or its absolute value) */
+    const int32_t* radii;       /* [E] */
+    const int64_t* gaussian_ids;/* packed: [nnz]; dense: NULL */
+    int32_t width, height;
+    float* grad2d;              /* [N] accumulated */
+    float* count;               /* [N] accumulated */
+    float* max_radii;           /* [N] or NULL */
+} tg_densify_stats_args;
+TG_API int tg_densify_stats(const tg_densify_stats_args* a, tg_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -278,3 +278,41 @@ def raster_bwd(means2d, M, colors, opacities, normals, textures, offsets, flatte
         _p(vn), _p(vd), _p(vm), int(mode), _p(o.v_means2d), _p(o.v_means2d_abs), _p(o.v_M), _p(o.v_colors),
         _p(o.v_opacities), _p(o.v_normals), _p(o.v_textures), _p(o.v_densify))
     return o
+
+
+# ---------------------------------------------------------------- gradient consumers (numpy)
+def selective_adam(param, grad, exp_avg, exp_avg_sq, visibility, lr, b1, b2, eps, dtype=np.float64):
+    """Selective Adam on rows of the first axis, restating textured_gaussians/cuda/csrc/adam.cu:29-44: rows with
+    visibility False are untouched; m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2, p += -lr m / (sqrt(v) + eps), no
+    bias correction.  The hyper-parameters are FP32 as in the reference's signature (adam.cu:25-28: const float lr,
+    b1, b2, eps), so 1 - b2 is 1 - fp32(b2) (exact in FP32).  Returns new (param, exp_avg, exp_avg_sq)."""
+    lr, b1, b2, eps = (float(np.float32(x)) for x in (lr, b1, b2, eps))
+    p, g, m, v = (np.array(x, dtype) for x in (param, grad, exp_avg, exp_avg_sq))
+    sel = np.asarray(visibility).reshape(-1).astype(bool)
+    m[sel] = b1 * m[sel] + (1.0 - b1) * g[sel]
+    v[sel] = b2 * v[sel] + (1.0 - b2) * g[sel] * g[sel]
+    p[sel] = p[sel] + (-lr * m[sel] / (np.sqrt(v[sel]) + eps))
+    return p, m, v
+
+
+def densify_stats(grads2d, radii, width, height, n_cameras, N, gaussian_ids=None, dtype=np.float64):
+    """Running densification statistics from zero, restating DefaultStrategy._update_state
+    (textured_gaussians/strategy/default.py:225-261): per entry with radius > 0 the norm of
+    (gx * width/2 * C, gy * height/2 * C) is added to grad2d[g], 1 to count[g], and max_radii[g] is the
+    maximum of radius / max(width, height) computed as an FP32 division, as the reference's torch division does
+    (a true maximum; the reference's indexed assignment keeps the last camera's value for a Gaussian seen by
+    several cameras).  Dense: [C,N] entries, packed: gaussian_ids."""
+    g = np.array(grads2d, dtype).reshape(-1, 2).copy()
+    r = np.asarray(radii).reshape(-1)
+    g[:, 0] *= width / 2.0 * n_cameras
+    g[:, 1] *= height / 2.0 * n_cameras
+    gid = (np.tile(np.arange(N), n_cameras) if gaussian_ids is None else np.asarray(gaussian_ids).reshape(-1))
+    sel = r > 0
+    grad2d = np.zeros(N, dtype)
+    count = np.zeros(N, dtype)
+    max_radii = np.zeros(N, np.float32)
+    np.add.at(grad2d, gid[sel], np.linalg.norm(g[sel], axis=-1))
+    np.add.at(count, gid[sel], 1.0)
+    frac = r[sel].astype(np.float32) / np.float32(max(width, height))
+    np.maximum.at(max_radii, gid[sel], frac)
+    return grad2d, count, max_radii

@@ -10,6 +10,7 @@ but these pure-torch twins import and run on the CPU:
   * _isect_offset_encode           textured_gaussians/cuda/_torch_impl.py:403-429
   * _spherical_harmonics           textured_gaussians/cuda/_torch_impl.py:704-714
   * accumulate_2dgs                textured_gaussians/cuda/_torch_impl_2dgs.py:78-168
+  * DefaultStrategy._update_state  textured_gaussians/strategy/default.py:213-261
 accumulate_2dgs needs two functions of the third-party package nerfacc
 (not installed): render_weight_from_alpha and accumulate_along_rays.  A
 stand-in module below restates their published semantics (nerfacc 0.5:
@@ -147,7 +148,39 @@ def main():
         opacities=s.opacities, viewmats=s.viewmats, Ks=s.Ks, width=s.width, height=s.height, near=s.near_plane,
         far=s.far_plane, colors=colors, tile_size=ts, pair_gaussian_ids=gi.numpy(), pair_pixel_ids=pi.numpy(),
         renders=renders.numpy(), alphas=alphas.numpy(), normals=rnormals.numpy())
+    densify_golden()
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
+
+
+def densify_golden():
+    """Running densification statistics of the reference's DefaultStrategy on seeded gradients and radii:
+    dense [C=3], dense [C=1] (where its radius statistic is a plain maximum) and packed."""
+    from textured_gaussians.strategy.default import DefaultStrategy
+
+    rng = np.random.default_rng(41)
+    W, H, N = 120, 90, 500
+    out = {}
+    for tag, C, packed in (("dense3", 3, False), ("dense1", 1, False), ("packed", 3, True)):
+        radii = rng.integers(0, 6, size=(C, N)).astype(np.int32) * (rng.uniform(size=(C, N)) < 0.7)
+        grads = rng.normal(size=(C, N, 2)).astype(np.float32) * 1e-3
+        if packed:
+            cam, gid = np.nonzero(radii > 0)
+            radii_in, grads_in = radii[cam, gid].astype(np.int32), grads[cam, gid]
+        else:
+            gid, radii_in, grads_in = None, radii.astype(np.int32), grads
+        g2 = torch.from_numpy(grads_in.copy()).requires_grad_()
+        g2.grad = torch.from_numpy(grads_in.copy())
+        strat = DefaultStrategy(refine_scale2d_stop_iter=1)
+        state = {"grad2d": None, "count": None, "radii": None}
+        info = {"width": W, "height": H, "n_cameras": C, "radii": torch.from_numpy(radii_in),
+                "gaussian_ids": None if gid is None else torch.from_numpy(gid.astype(np.int64)),
+                strat.key_for_gradient: g2}
+        strat._update_state({"means": torch.zeros(N, 3)}, state, info, packed=packed)
+        out.update({f"{tag}_radii": radii_in, f"{tag}_grads": grads_in, f"{tag}_grad2d": state["grad2d"].numpy(),
+                    f"{tag}_count": state["count"].numpy(), f"{tag}_max_radii": state["radii"].numpy()})
+        if gid is not None:
+            out[f"{tag}_gaussian_ids"] = gid.astype(np.int64)
+    np.savez_compressed(os.path.join(HERE, "densify_stats.npz"), width=W, height=H, N=N, **out)
 
 
 if __name__ == "__main__":

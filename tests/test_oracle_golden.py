@@ -92,3 +92,18 @@ def test_sort_is_stable_on_the_reference_bit_range():
     for d in range(8):
         sel = (k & 7) == d
         assert (np.diff(v[sel]) > 0).all()  # equal keys keep emission order
+
+
+def test_densify_stats_oracle_matches_reference_update_state():
+    """Oracle of the densification statistics against the reference's own DefaultStrategy._update_state
+    (fixture tests/golden/densify_stats.npz): grad2d and count in every layout; the radius statistic where the
+    reference's indexed assignment is a plain maximum (one camera)."""
+    d = np.load(os.path.join(HERE, "densify_stats.npz"))
+    W, H, N = int(d["width"]), int(d["height"]), int(d["N"])
+    for tag, C in (("dense3", 3), ("dense1", 1), ("packed", 3)):
+        gid = d[f"{tag}_gaussian_ids"] if f"{tag}_gaussian_ids" in d.files else None
+        g2, cnt, mr = O.densify_stats(d[f"{tag}_grads"], d[f"{tag}_radii"], W, H, C, N, gaussian_ids=gid)
+        np.testing.assert_allclose(g2, d[f"{tag}_grad2d"], rtol=1e-5, atol=1e-7)
+        np.testing.assert_array_equal(cnt, d[f"{tag}_count"])
+        if tag == "dense1":
+            np.testing.assert_array_equal(mr, d[f"{tag}_max_radii"])

@@ -57,6 +57,11 @@ class ProjectPackedBwdArgs(ctypes.Structure):
                 ("sh_coeffs", P), ("v_colors", P), ("v_sh_coeffs", P)]
 
 
+class DensifyStatsArgs(ctypes.Structure):
+    _fields_ = [("C", I32), ("N", I64), ("n_elems", I64), ("grads2d", P), ("radii", P), ("gaussian_ids", P),
+                ("width", I32), ("height", I32), ("grad2d", P), ("count", P), ("max_radii", P)]
+
+
 class IsectArgs(ctypes.Structure):
     _fields_ = [("n_elems", I64), ("N", I64), ("camera_ids", P), ("means2d", P), ("radii", P), ("depths", P),
                 ("tile_size", I32), ("tile_width", I32), ("tile_height", I32), ("n_cameras", I32),
@@ -119,6 +124,8 @@ def lib() -> ctypes.CDLL:
                 ("tg_rasterize_fwd", [ctypes.POINTER(RasterFwdArgs), P]),
                 ("tg_rasterize_bwd", [ctypes.POINTER(RasterBwdArgs), P]),
                 ("tg_sh_fwd", [I64, I64, I32, I32, P, P, P, P, P]),
+                ("tg_selective_adam", [P, P, P, P, P, F32, F32, F32, F32, I64, I64, I32, P, P]),
+                ("tg_densify_stats", [ctypes.POINTER(DensifyStatsArgs), P]),
                 ("tg_sh_bwd", [I64, I64, I32, I32, P, P, P, P, P, P, P]),
             ]:
                 fn = getattr(L, name)

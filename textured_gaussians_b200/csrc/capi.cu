@@ -40,6 +40,10 @@ cudaError_t launch_sh_fwd(int64_t n, int64_t rows, int degree, int K, const floa
 cudaError_t launch_sh_bwd(int64_t n, int64_t rows, int degree, int K, const float* dirs, const float* coeffs,
                           const uint8_t* masks, const float* v_colors, float* v_coeffs, float* v_dirs,
                           cudaStream_t s);
+cudaError_t launch_selective_adam(float* param, const float* grad, float* m, float* v, const uint8_t* vis, float lr,
+                                  float b1, float b2, float eps, int64_t N, int64_t M, int shadow_format, void* shadow,
+                                  cudaStream_t s);
+cudaError_t launch_densify_stats(const tg_densify_stats_args& a, cudaStream_t s);
 int fail_with(int code, const char* msg);
 }  // namespace tg
 
@@ -437,6 +441,29 @@ int tg_sh_bwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, const fl
     return cuda_status(
         tg::launch_sh_bwd(n, coeff_rows, degree, K, dirs, coeffs, masks, v_colors, v_coeffs, v_dirs, stream),
         "tg_sh_bwd");
+}
+
+int tg_selective_adam(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, const uint8_t* visibility,
+                      float lr, float b1, float b2, float eps, int64_t N, int64_t M, int32_t shadow_format,
+                      void* shadow, tg_stream_t stream) {
+    TG_REQUIRE(N >= 0 && M >= 0, TG_ERR_INVALID_ARG, "negative sizes");
+    TG_REQUIRE(shadow_format == TG_TEX_NONE || shadow_format == TG_TEX_BF16 || shadow_format == TG_TEX_F16,
+               TG_ERR_UNSUPPORTED, "shadow format %d not supported (none, BF16, FP16)", shadow_format);
+    if (N * M == 0) return TG_OK;
+    TG_REQUIRE(param && grad && exp_avg && exp_avg_sq && visibility, TG_ERR_INVALID_ARG, "null pointer");
+    TG_REQUIRE(shadow_format == TG_TEX_NONE || shadow != nullptr, TG_ERR_INVALID_ARG, "null shadow");
+    return cuda_status(tg::launch_selective_adam(param, grad, exp_avg, exp_avg_sq, visibility, lr, b1, b2, eps, N, M,
+                                                 shadow_format, shadow, stream),
+                       "tg_selective_adam");
+}
+
+int tg_densify_stats(const tg_densify_stats_args* a, tg_stream_t stream) {
+    TG_REQUIRE(a != nullptr, TG_ERR_INVALID_ARG, "null args");
+    TG_REQUIRE(a->C >= 0 && a->N >= 0 && a->n_elems >= 0 && a->width > 0 && a->height > 0, TG_ERR_INVALID_ARG,
+               "bad sizes");
+    if (a->N == 0 || (a->gaussian_ids && a->n_elems == 0) || (!a->gaussian_ids && a->C == 0)) return TG_OK;
+    TG_REQUIRE(a->grads2d && a->radii && a->grad2d && a->count, TG_ERR_INVALID_ARG, "null pointer");
+    return cuda_status(tg::launch_densify_stats(*a, stream), "tg_densify_stats");
 }
 
 }  // extern "C"

@@ -1,5 +1,6 @@
 """Op surface mirroring textured_gaussians.cuda (see _wrapper.py)."""
 from ._wrapper import (
+    densify_stats,
     fully_fused_projection_2dgs,
     isect_offset_encode,
     isect_offset_encode_views,
@@ -7,6 +8,7 @@ from ._wrapper import (
     make_texture_storage,
     rasterize_to_pixels_2dgs,
     rasterize_to_pixels_textured_gaussians,
+    selective_adam_update,
     sort_pairs,
     spherical_harmonics,
     spherical_harmonics_shared,
@@ -14,6 +16,7 @@ from ._wrapper import (
 )
 
 __all__ = [
+    "densify_stats",
     "fully_fused_projection_2dgs",
     "isect_offset_encode",
     "isect_offset_encode_views",
@@ -21,6 +24,7 @@ __all__ = [
     "make_texture_storage",
     "rasterize_to_pixels_2dgs",
     "rasterize_to_pixels_textured_gaussians",
+    "selective_adam_update",
     "sort_pairs",
     "spherical_harmonics",
     "spherical_harmonics_shared",

@@ -873,3 +873,53 @@ def rasterize_to_pixels_2dgs(
     if padded > 0:
         render_colors = render_colors[..., :-padded]
     return (render_colors,) + tuple(out[1:])
+
+
+# --------------------------------------------------------------------------- gradient consumers
+_SHADOW_FORMAT = {None: B.TG_TEX_NONE, torch.bfloat16: B.TG_TEX_BF16, torch.float16: B.TG_TEX_F16}
+
+
+@torch.no_grad()
+def selective_adam_update(param: Tensor, param_grad: Tensor, exp_avg: Tensor, exp_avg_sq: Tensor,
+                          tiles_touched: Tensor, lr: float, b1: float, b2: float, eps: float, N: int, M: int, *,
+                          shadow: Optional[Tensor] = None) -> None:
+    """Adam step on the rows whose ``tiles_touched`` flag is set (reference: cuda/_wrapper.py:26-40,
+    csrc/adam.cu:17-45; no bias correction).  ``shadow`` (BF16 / FP16, same number of elements) receives the
+    updated rows in the same pass, e.g. the low-precision texture storage the compositor samples."""
+    for t in (param, param_grad, exp_avg, exp_avg_sq):
+        assert t.dtype == torch.float32 and t.is_contiguous() and t.numel() == N * M, (t.dtype, t.shape)
+    vis = tiles_touched.reshape(-1)
+    assert vis.numel() == N, vis.shape
+    vis = vis.to(torch.uint8).contiguous()
+    if shadow is not None:
+        assert shadow.dtype in (torch.bfloat16, torch.float16) and shadow.is_contiguous() and shadow.numel() == N * M
+    fmt = _SHADOW_FORMAT[None if shadow is None else shadow.dtype]
+    st = B.stream_of(param)
+    B.call("tg_selective_adam", st, B.lib().tg_selective_adam, B.ptr(param), B.ptr(param_grad), B.ptr(exp_avg),
+           B.ptr(exp_avg_sq), B.ptr(vis), float(lr), float(b1), float(b2), float(eps), int(N), int(M), fmt,
+           B.ptr(shadow), st)
+
+
+@torch.no_grad()
+def densify_stats(grads2d: Tensor, radii: Tensor, width: int, height: int, n_cameras: int, grad2d: Tensor,
+                  count: Tensor, max_radii: Optional[Tensor] = None, gaussian_ids: Optional[Tensor] = None) -> None:
+    """Running densification statistics in place (reference: strategy/default.py:213-261): per entry with
+    radius > 0, ``grad2d[g] += |grad * (width/2 * C, height/2 * C)|``, ``count[g] += 1`` and
+    ``max_radii[g] = max(max_radii[g], radius / max(width, height))``.  Dense inputs are [C,N,...];
+    packed ones [nnz,...] with ``gaussian_ids``."""
+    N = grad2d.numel()
+    grads2d = grads2d.float().contiguous()
+    radii = radii.int().contiguous()
+    for t in (grad2d, count) + (() if max_radii is None else (max_radii,)):
+        assert t.dtype == torch.float32 and t.is_contiguous() and t.numel() == N
+    if gaussian_ids is None:
+        assert radii.shape == (n_cameras, N) and grads2d.shape == (n_cameras, N, 2), (radii.shape, grads2d.shape)
+        E = n_cameras * N
+    else:
+        E = radii.numel()
+        gaussian_ids = gaussian_ids.to(torch.int64).contiguous()
+        assert gaussian_ids.shape == (E,) and grads2d.shape == (E, 2)
+    a = B.DensifyStatsArgs(int(n_cameras), N, E, B.ptr(grads2d), B.ptr(radii), B.ptr(gaussian_ids), int(width),
+                           int(height), B.ptr(grad2d), B.ptr(count), B.ptr(max_radii))
+    st = B.stream_of(grad2d)
+    B.call("tg_densify_stats", st, B.lib().tg_densify_stats, ctypes.byref(a), st)
