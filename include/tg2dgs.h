@@ -370,6 +370,15 @@ typedef struct {
      * CTAs as fit on the device takes work items (tiles, in tile_order) from
      * it until none is left.  NULL: one CTA per work item. */
     uint32_t* work_queue;
+    /* The mipmapped2 filter (mip_levels = L > 0; rasterize_to_pixels_mip2_
+     * textured_gaussians_2dgs_fwd.cu of the reference): textures are 2^L x 2^L
+     * (tex_ry = tex_rx = 2^L) and tex_coarse holds their coarser levels,
+     * [G, (4^L - 1) / 3, 4] FP32 in the reference's pyramid order (coarsest
+     * first, as made by tg_generate_mipmap); level 0 is read from `textures`.
+     * Supported with F32 / BF16 storage, 3 or 4 channels, tile 8 or 16, no
+     * persistent launch, and the reference adjoint. */
+    int32_t mip_levels;
+    const float* tex_coarse;
 } tg_raster_fwd_args;
 TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
 
@@ -400,6 +409,7 @@ typedef struct {
     float* v_normals;            /* [E,3] */
     float* v_textures;           /* [G,ry,rx,4] FP32 or NULL */
     float* v_densify;            /* [E,2] */
+    float* v_tex_coarse;         /* mipmapped2: [G, (4^L - 1) / 3, 4] gradient of tex_coarse (zeroed by the call) */
 } tg_raster_bwd_args;
 TG_API int tg_rasterize_bwd(const tg_raster_bwd_args* a, tg_stream_t stream);
 
@@ -416,6 +426,19 @@ TG_API int tg_sh_fwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, c
                      const uint8_t* masks, float* colors, tg_stream_t stream);
 TG_API int tg_sh_bwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, const float* dirs, const float* coeffs,
                      const uint8_t* masks, const float* v_colors, float* v_coeffs, float* v_dirs, tg_stream_t stream);
+
+/* ------------------------------------------------------------------ mip pyramid
+ * Replaces generate_mipmap_fwd / generate_mipmap_bwd
+ * (textured_gaussians/cuda/csrc/generate_mipmap_{fwd,bwd}.cu): coarse[g] holds
+ * levels 1..L of the 2^L x 2^L RGBA texture g, coarsest first (level t, side
+ * 2^(L-t), starts at texel (4^(L-t) - 1) / 3), each texel the mean of its
+ * four children summed in the reference's order ((a + b) + c) + d, then / 4.
+ * The reference also copies level 0 into its pyramid; here the compositor
+ * reads level 0 from the texture storage itself.  The adjoint adds each coarse
+ * gradient / 4 into its four children, coarsest to finest, ending in
+ * v_textures (accumulated, not overwritten); v_coarse is modified in place. */
+TG_API int tg_generate_mipmap(const float* textures, float* coarse, int64_t G, int32_t L, tg_stream_t stream);
+TG_API int tg_generate_mipmap_bwd(float* v_coarse, float* v_textures, int64_t G, int32_t L, tg_stream_t stream);
 
 /* ------------------------------------------------------------------ gradient consumers
  * Replaces selective_adam_update (textured_gaussians/cuda/csrc/adam.cu:17-89):

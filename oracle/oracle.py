@@ -47,10 +47,11 @@ def lib():
             getattr(_LIB, f"tgo_sh_fwd_{suf}").argtypes = [c_i64, c_int, c_int] + [c_ptr] * 4
             getattr(_LIB, f"tgo_sh_bwd_{suf}").argtypes = [c_i64, c_int, c_int] + [c_ptr] * 6
             getattr(_LIB, f"tgo_raster_fwd_{suf}").argtypes = (
-                [c_int] * 8 + [c_i64] + [c_ptr] * 6 + [c_int, c_int, c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl, c_dbl] + [c_ptr] * 11
+                [c_int] * 8 + [c_i64] + [c_ptr] * 6 + [c_int, c_int, c_int, c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl, c_dbl]
+                + [c_ptr] * 11
             )
             getattr(_LIB, f"tgo_raster_bwd_{suf}").argtypes = (
-                [c_int] * 8 + [c_i64, c_i64] + [c_ptr] * 6 + [c_int, c_int, c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl]
+                [c_int] * 8 + [c_i64, c_i64] + [c_ptr] * 6 + [c_int, c_int, c_int, c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl]
                 + [c_ptr] * 9 + [c_int] + [c_ptr] * 8
             )
         _LIB.tgo_sort_pairs.argtypes = [c_i64, c_ptr, c_ptr, c_int]
@@ -199,13 +200,63 @@ class RasterFwdOut:
     branch_sig: np.ndarray
 
 
+def _tex_shape(textures, mip_levels):
+    if textures is None:
+        return 0, 0
+    if mip_levels:
+        assert textures.ndim == 3 and textures.shape[1] == (4 ** (mip_levels + 1) - 1) // 3, "expects the full pyramid"
+        return 1 << mip_levels, 1 << mip_levels
+    return textures.shape[1], textures.shape[2]
+
+
+def mip_level_base(L: int, t: int) -> int:
+    """Texel index of level t (side 2^(L-t)) in the pyramid of a 2^L texture, coarsest first (filters/mip2.cuh:15-25)."""
+    return (4 ** (L - t) - 1) // 3
+
+
+def generate_mipmap(textures):
+    """Full mip pyramid [G, (4^(L+1)-1)/3, 4] of square 2^L textures [G, R, R, 4], restating
+    generate_mipmap_fwd.cu:19-57: level 0 is the texture itself; a texel of level t is ((a + b) + c + d) / 4 of its
+    four children at level t - 1 (row-major order), in the textures' dtype."""
+    G, R = textures.shape[0], textures.shape[1]
+    L = R.bit_length() - 1
+    assert textures.shape[2] == R and R == 1 << L
+    out = np.empty((G, (4 ** (L + 1) - 1) // 3, textures.shape[3]), textures.dtype)
+    lvl = np.ascontiguousarray(textures)
+    out[:, mip_level_base(L, 0):] = lvl.reshape(G, R * R, -1)
+    four = textures.dtype.type(4)
+    for t in range(1, L + 1):
+        lvl = (lvl[:, 0::2, 0::2] + lvl[:, 0::2, 1::2] + lvl[:, 1::2, 0::2] + lvl[:, 1::2, 1::2]) / four
+        side = R >> t
+        out[:, mip_level_base(L, t):mip_level_base(L, t) + side * side] = lvl.reshape(G, side * side, -1)
+    return out
+
+
+def generate_mipmap_bwd(v_pyramid, L: int):
+    """Texture gradient [G, R, R, 4] from the full pyramid's, restating generate_mipmap_bwd.cu:19-60: coarsest first,
+    each child adds its parent's (already complete) gradient / 4."""
+    v = np.array(v_pyramid)
+    G, four = v.shape[0], v.dtype.type(4)
+    for t in range(L, 0, -1):
+        side = 1 << (L - t)
+        par = v[:, mip_level_base(L, t):mip_level_base(L, t) + side * side].reshape(G, side, side, -1) / four
+        cb = mip_level_base(L, t - 1)
+        ch = v[:, cb:cb + 4 * side * side].reshape(G, side, 2, side, 2, -1)
+        ch += par[:, :, None, :, None, :]
+        v[:, cb:cb + 4 * side * side] = ch.reshape(G, 4 * side * side, -1)
+    R = 1 << L
+    return v[:, mip_level_base(L, 0):].reshape(G, R, R, -1)
+
+
 def raster_fwd(means2d, M, colors, opacities, normals, textures, offsets, flatten_ids, W, H, tile_size,
                range_x=3.0, range_y=3.0, backgrounds=None, masks=None, gaussian_ids=None, n_gauss=None,
-               contrib_threshold=0.0, g_weight=1.0, dtype=np.float32):
+               contrib_threshold=0.0, g_weight=1.0, mip_levels=0, dtype=np.float32):
     """Compositor forward.  ``textures=None`` selects the plain 2DGS compositor.
 
     Dense layout: means2d [C,N,2] ...; packed layout: [nnz,...] plus
-    ``gaussian_ids`` [nnz] and ``n_gauss``.
+    ``gaussian_ids`` [nnz] and ``n_gauss``.  ``mip_levels`` L > 0 selects the
+    mipmapped2 filter on a 2^L x 2^L texture: ``textures`` is then the full
+    pyramid [G, (4^(L+1)-1)/3, 4] of :func:`generate_mipmap`.
     """
     means2d, M, colors, opacities, normals, textures, backgrounds = (
         _c(x, dtype) for x in (means2d, M, colors, opacities, normals, textures, backgrounds))
@@ -218,7 +269,7 @@ def raster_fwd(means2d, M, colors, opacities, normals, textures, offsets, flatte
     G = N if gaussian_ids is None else n_gauss
     gid = None if gaussian_ids is None else np.ascontiguousarray(gaussian_ids, np.int64)
     m = None if masks is None else np.ascontiguousarray(masks, np.uint8)
-    ry, rx = (textures.shape[1], textures.shape[2]) if textures is not None else (0, 0)
+    ry, rx = _tex_shape(textures, mip_levels)
     o = RasterFwdOut(
         colors=np.zeros((C, H, W, D), dtype), alphas=np.zeros((C, H, W, 1), dtype), normals=np.zeros((C, H, W, 3), dtype),
         distort=np.zeros((C, H, W, 1), dtype), median=np.zeros((C, H, W, 1), dtype),
@@ -227,8 +278,8 @@ def raster_fwd(means2d, M, colors, opacities, normals, textures, offsets, flatte
         branch_sig=np.zeros((C, H, W), np.uint64))
     getattr(lib(), f"tgo_raster_fwd_{_suf(dtype)}")(
         C, N, D, int(W), int(H), tile_size, tw, th, flatten_ids.size, _p(means2d), _p(M), _p(colors), _p(opacities),
-        _p(normals), _p(textures), ry, rx, float(range_x), float(range_y), _p(backgrounds), _p(m), _p(offsets),
-        _p(flatten_ids), _p(gid), float(contrib_threshold), float(g_weight), _p(o.colors), _p(o.alphas),
+        _p(normals), _p(textures), ry, rx, int(mip_levels), float(range_x), float(range_y), _p(backgrounds), _p(m),
+        _p(offsets), _p(flatten_ids), _p(gid), float(contrib_threshold), float(g_weight), _p(o.colors), _p(o.alphas),
         _p(o.normals), _p(o.distort), _p(o.median), _p(o.last_ids), _p(o.median_ids), _p(o.contrib_sum),
         _p(o.contrib_count), _p(o.pair_count), _p(o.branch_sig))
     return o
@@ -248,8 +299,9 @@ class RasterBwdOut:
 
 def raster_bwd(means2d, M, colors, opacities, normals, textures, offsets, flatten_ids, W, H, tile_size, fwd,
                v_colors, v_alphas, v_normals, v_distort, v_median, range_x=3.0, range_y=3.0, backgrounds=None,
-               masks=None, gaussian_ids=None, n_gauss=None, g_weight=1.0, mode=0, dtype=np.float32):
-    """Compositor adjoint.  mode 0: reference "bilinear", 1: "bilinear_bwd2", 2: exact."""
+               masks=None, gaussian_ids=None, n_gauss=None, g_weight=1.0, mode=0, mip_levels=0, dtype=np.float32):
+    """Compositor adjoint.  mode 0: reference "bilinear", 1: "bilinear_bwd2", 2: exact.  With ``mip_levels`` > 0
+    (mipmapped2, mode 0 only, as the reference has no other) ``v_textures`` is the full pyramid's gradient."""
     means2d, M, colors, opacities, normals, textures, backgrounds = (
         _c(x, dtype) for x in (means2d, M, colors, opacities, normals, textures, backgrounds))
     offsets = np.ascontiguousarray(offsets, np.int32)
@@ -261,7 +313,7 @@ def raster_bwd(means2d, M, colors, opacities, normals, textures, offsets, flatte
     E = means2d.shape[0] if packed else C * N
     gid = None if gaussian_ids is None else np.ascontiguousarray(gaussian_ids, np.int64)
     m = None if masks is None else np.ascontiguousarray(masks, np.uint8)
-    ry, rx = (textures.shape[1], textures.shape[2]) if textures is not None else (0, 0)
+    ry, rx = _tex_shape(textures, mip_levels)
     fc, fa = _c(fwd.colors, dtype), _c(fwd.alphas, dtype)
     li, mi = np.ascontiguousarray(fwd.last_ids, np.int32), np.ascontiguousarray(fwd.median_ids, np.int32)
     vc, va, vn, vd, vm = (_c(x, dtype) for x in (v_colors, v_alphas, v_normals, v_distort, v_median))
@@ -273,7 +325,7 @@ def raster_bwd(means2d, M, colors, opacities, normals, textures, offsets, flatte
         v_densify=np.zeros(means2d.shape, dtype))
     getattr(lib(), f"tgo_raster_bwd_{_suf(dtype)}")(
         C, N, D, int(W), int(H), tile_size, tw, th, flatten_ids.size, E, _p(means2d), _p(M), _p(colors),
-        _p(opacities), _p(normals), _p(textures), ry, rx, float(range_x), float(range_y), _p(backgrounds), _p(m),
+        _p(opacities), _p(normals), _p(textures), ry, rx, int(mip_levels), float(range_x), float(range_y), _p(backgrounds), _p(m),
         _p(offsets), _p(flatten_ids), _p(gid), float(g_weight), _p(fc), _p(fa), _p(li), _p(mi), _p(vc), _p(va),
         _p(vn), _p(vd), _p(vm), int(mode), _p(o.v_means2d), _p(o.v_means2d_abs), _p(o.v_M), _p(o.v_colors),
         _p(o.v_opacities), _p(o.v_normals), _p(o.v_textures), _p(o.v_densify))

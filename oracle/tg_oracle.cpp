@@ -372,17 +372,60 @@ template <typename T> struct RasterIn {
     const int32_t* flatten_ids;
     const int64_t* gaussian_ids;  // packed: [nnz] texture row of each element, else null (row = e % N)
     T contrib_threshold, g_weight;
+    int mip_L;  // 0: bilinear on [G,ry,rx,4]; L > 0: mipmapped2 on the full pyramid [G,(4^(L+1)-1)/3,4]
 };
 
 template <typename T> inline int64_t tex_row(const RasterIn<T>& a, int64_t e) {
     return a.gaussian_ids ? a.gaussian_ids[e] : e % a.N;
 }
 
+// texels per splat row of the texture array
+template <typename T> inline int64_t tex_texels(const RasterIn<T>& a) {
+    return a.mip_L > 0 ? ((int64_t(1) << (2 * (a.mip_L + 1))) - 1) / 3 : (int64_t)a.tex_ry * a.tex_rx;
+}
+
+// mipmapped2 taps, restating filters/mip2.cuh:27-105 (pyramid coordinate of level t of a 2^L texture:
+// (4^(L-t) - 1) / 3, coarsest first); a level beyond the coarsest is treated as invalid.
+template <typename T>
+inline int mip2_taps(T sx, T sy, T dxx, T dxy, T dyx, T dyy, int R, int L, T xr, T yr, int64_t (&mc)[8], T (&w)[8]) {
+    const T fr = T(R - 1);
+    const T ax = dxx / (xr * 2) * fr, ay = dxy / (xr * 2) * fr;
+    const T bx = dyx / (yr * 2) * fr, by = dyy / (yr * 2) * fr;
+    const T duv = std::max(std::sqrt(ax * ax + ay * ay), std::sqrt(bx * bx + by * by));
+    T t = std::log2(duv);
+    if (t < 0) t = 0;
+    else if (t > 31) t = 31;
+    const T u = (sx + xr) / (xr * 2) * fr, v = (sy + yr) / (yr * 2) * fr;
+    // a NaN level converts to level 0 (the GPU's float -> int conversion); its weights stay NaN
+    const int tl = t == t ? (int)std::floor(t) : 0, th = t == t ? (int)std::ceil(t) : 0;
+    if (th > L) return -1;
+    const T sl = T(1u << tl), sh = T(1u << th);
+    const T us = (u + T(0.5)) / sl - T(0.5), ug = (u + T(0.5)) / sh - T(0.5);
+    const T vs = (v + T(0.5)) / sl - T(0.5), vg = (v + T(0.5)) / sh - T(0.5);
+    const int uls = (int)std::floor(us), ulg = (int)std::floor(ug), vls = (int)std::floor(vs), vlg = (int)std::floor(vg);
+    const int uhs = (int)std::ceil(us), uhg = (int)std::ceil(ug), vhs = (int)std::ceil(vs), vhg = (int)std::ceil(vg);
+    if (uls < 0 || ulg < 0 || vls < 0 || vlg < 0 || uhs > ((R - 1) >> tl) || uhg > ((R - 1) >> th) ||
+        vhs > ((R - 1) >> tl) || vhg > ((R - 1) >> th))
+        return -1;
+    const int64_t rl = R >> tl, rh = R >> th;
+    const int64_t bl = ((int64_t(1) << (2 * (L - tl))) - 1) / 3, bh = ((int64_t(1) << (2 * (L - th))) - 1) / 3;
+    mc[0] = bl + vls * rl + uls; mc[1] = bl + vls * rl + uhs; mc[2] = bl + vhs * rl + uls; mc[3] = bl + vhs * rl + uhs;
+    mc[4] = bh + vlg * rh + ulg; mc[5] = bh + vlg * rh + uhg; mc[6] = bh + vhg * rh + ulg; mc[7] = bh + vhg * rh + uhg;
+    const T wus = us - T(uls), wvs = vs - T(vls), wug = ug - T(ulg), wvg = vg - T(vlg), wt = t - T(tl);
+    w[0] = (1 - wus) * (1 - wvs) * (1 - wt); w[1] = wus * (1 - wvs) * (1 - wt);
+    w[2] = (1 - wus) * wvs * (1 - wt);       w[3] = wus * wvs * (1 - wt);
+    w[4] = (1 - wug) * (1 - wvg) * wt;       w[5] = wug * (1 - wvg) * wt;
+    w[6] = (1 - wug) * wvg * wt;             w[7] = wug * wvg * wt;
+    return 1;
+}
+
 template <typename T> struct SplatEval {
     bool valid;
     int valid_tex;
-    int uc[4], vc[4];
-    T w[4];
+    int uc[4], vc[4];  // bilinear texel coordinates
+    int nt;            // taps: 4 bilinear, 8 mipmapped2
+    int64_t ti[8];     // texel index of each tap within the splat's row
+    T w[8];
     T asf, g3, g2, kern, vis, alpha;
     V3<T> hu, hv, zeta;
     T sx, sy, dx, dy;
@@ -399,16 +442,38 @@ inline void eval_splat(const RasterIn<T>& a, int64_t g, T px, T py, SplatEval<T>
     e.zeta = cross3(e.hu, e.hv);
     e.valid = true;
     e.valid_tex = -1;
+    e.nt = 4;
     if (e.zeta.z == T(0)) { e.valid = false; return; }
     e.sx = e.zeta.x / e.zeta.z;
     e.sy = e.zeta.y / e.zeta.z;
     const T opac = a.opacities[g];
+    if (a.textures && a.mip_L > 0) {
+        // mipmapped2 (mip2 fwd.cu:293-347): s at the pixel's edge midpoints gives the footprint
+        const V3<T> hw = T(0.5) * M2;
+        const V3<T> cx0 = cross3(e.hu - hw, e.hv), cx1 = cross3(e.hu + hw, e.hv);
+        const V3<T> cy0 = cross3(e.hu, e.hv - hw), cy1 = cross3(e.hu, e.hv + hw);
+        if (cx0.z == T(0) || cx1.z == T(0) || cy0.z == T(0) || cy1.z == T(0)) {
+            e.valid = false;
+            e.g3 = e.g2 = T(0);
+            return;
+        }
+        e.nt = 8;
+        e.valid_tex = mip2_taps<T>(e.sx, e.sy, cx1.x / cx1.z - cx0.x / cx0.z, cx1.y / cx1.z - cx0.y / cx0.z,
+                                   cy1.x / cy1.z - cy0.x / cy0.z, cy1.y / cy1.z - cy0.y / cy0.z, a.tex_rx, a.mip_L,
+                                   a.range_x, a.range_y, e.ti, e.w);
+    } else if (a.textures) {
+        T w4[4];
+        e.valid_tex = bilinear_taps<T>(e.sx, e.sy, a.tex_rx, a.tex_ry, a.range_x, a.range_y, e.uc, e.vc, w4);
+        for (int i = 0; i < 4; ++i) {
+            e.w[i] = w4[i];
+            e.ti[i] = (int64_t)e.vc[i] * a.tex_rx + e.uc[i];
+        }
+    }
     if (a.textures) {
-        e.valid_tex = bilinear_taps<T>(e.sx, e.sy, a.tex_rx, a.tex_ry, a.range_x, a.range_y, e.uc, e.vc, e.w);
         if (e.valid_tex > 0) {
-            const T* tex = a.textures + tex_row(a, g) * (int64_t)a.tex_ry * a.tex_rx * 4;
+            const T* tex = a.textures + tex_row(a, g) * tex_texels(a) * 4;
             e.asf = 0;
-            for (int i = 0; i < 4; ++i) e.asf += e.w[i] * tex[((int64_t)e.vc[i] * a.tex_rx + e.uc[i]) * 4 + 3];
+            for (int i = 0; i < e.nt; ++i) e.asf += e.w[i] * tex[e.ti[i] * 4 + 3];
         } else {
             e.asf = 1;
         }
@@ -434,9 +499,9 @@ inline void eval_splat(const RasterIn<T>& a, int64_t g, T px, T py, SplatEval<T>
 template <typename T> inline T tex_channel(const RasterIn<T>& a, int64_t g, const SplatEval<T>& e, int k) {
     // texture channel k for colour channel k; channels >= 4 have no texture term
     if (k >= 4 || e.valid_tex <= 0) return T(0);
-    const T* tex = a.textures + tex_row(a, g) * (int64_t)a.tex_ry * a.tex_rx * 4;
+    const T* tex = a.textures + tex_row(a, g) * tex_texels(a) * 4;
     T s = 0;
-    for (int i = 0; i < 4; ++i) s += e.w[i] * tex[((int64_t)e.vc[i] * a.tex_rx + e.uc[i]) * 4 + k];
+    for (int i = 0; i < e.nt; ++i) s += e.w[i] * tex[e.ti[i] * 4 + k];
     return s;
 }
 
@@ -503,7 +568,7 @@ void raster_fwd(const RasterIn<T>& a, const RasterOut<T>& o, int32_t* pair_count
                             mix(e.g3 <= e.g2 ? 3 : 4);
                             mix((uint64_t)(e.valid_tex + 2));
                             if (e.valid_tex > 0)
-                                for (int q = 0; q < 4; ++q) mix((uint64_t)(e.uc[q] * 4099 + e.vc[q]));
+                                for (int q = 0; q < e.nt; ++q) mix((uint64_t)e.ti[q]);
                             const T op = a.opacities[g];
                             mix(a.textures ? (op * e.vis * e.asf <= T(0.999) ? 5 : 6) : (op * e.vis <= T(0.999) ? 5 : 6));
                         }
@@ -619,14 +684,14 @@ void raster_bwd(const RasterIn<T>& a, const RasterGradIn<T>& gi, const RasterGra
                     Tr *= ra;
                     const T fac = e.alpha * Tr;
                     const bool tex_on = a.textures && e.valid_tex > 0;
-                    T* vtex = tex_on ? go.v_textures + tex_row(a, g) * (int64_t)a.tex_ry * a.tex_rx * 4 : nullptr;
-                    const T* tex = tex_on ? a.textures + tex_row(a, g) * (int64_t)a.tex_ry * a.tex_rx * 4 : nullptr;
+                    T* vtex = tex_on ? go.v_textures + tex_row(a, g) * tex_texels(a) * 4 : nullptr;
+                    const T* tex = tex_on ? a.textures + tex_row(a, g) * tex_texels(a) * 4 : nullptr;
                     for (int k = 0; k < D; ++k) {
                         vrgb[k] += fac * vc[k];
                         texc[k] = 0;
                         if (tex_on && k < 4)
-                            for (int t = 0; t < 4; ++t) {
-                                const int64_t o = ((int64_t)e.vc[t] * a.tex_rx + e.uc[t]) * 4 + k;
+                            for (int t = 0; t < e.nt; ++t) {
+                                const int64_t o = e.ti[t] * 4 + k;
                                 atomic_add(vtex + o, fac * e.w[t] * vc[k]);
                                 texc[k] += e.w[t] * tex[o];
                             }
@@ -675,12 +740,9 @@ void raster_bwd(const RasterIn<T>& a, const RasterGradIn<T>& gi, const RasterGra
                         }
                         v_op = a.textures ? e.vis * v_alpha * e.asf : e.vis * v_alpha;
                         if (tex_on)
-                            for (int t = 0; t < 4; ++t) {
-                                const int64_t o = ((int64_t)e.vc[t] * a.tex_rx + e.uc[t]) * 4 + 3;
-                                atomic_add(vtex + o, e.w[t] * e.vis * opac * v_alpha);
-                            }
+                            for (int t = 0; t < e.nt; ++t) atomic_add(vtex + e.ti[t] * 4 + 3, e.w[t] * e.vis * opac * v_alpha);
                     }
-                    if (mode >= 1 && tex_on) {
+                    if (mode >= 1 && tex_on && a.mip_L == 0) {
                         const T wu = e.w[1] + e.w[3], wv = e.w[2] + e.w[3];
                         const T dbu[4] = {-(T(1) - wv), T(1) - wv, -wv, wv};
                         const T dbv[4] = {-(T(1) - wu), -wu, T(1) - wu, wu};
@@ -884,13 +946,13 @@ void sh_bwd(int64_t n, int degree, int K, const T* dirs, const T* coeffs, const 
     TGO_EXPORT void tgo_raster_fwd_##SUF(                                                                            \
         int C, int N, int D, int W, int H, int tile_size, int tile_w, int tile_h, int64_t n_isects, const T* means2d, \
         const T* M, const T* colors, const T* opacities, const T* normals, const T* textures, int tex_ry, int tex_rx, \
-        double range_x, double range_y, const T* backgrounds, const uint8_t* masks, const int32_t* offsets,           \
+        int mip_L, double range_x, double range_y, const T* backgrounds, const uint8_t* masks, const int32_t* offsets, \
         const int32_t* flatten_ids, const int64_t* gaussian_ids, double contrib_threshold, double g_weight,           \
         T* out_colors, T* out_alphas, T* out_normals, T* out_distort, T* out_median, int32_t* last_ids,              \
         int32_t* median_ids, T* contrib_sum, T* contrib_count, int32_t* pair_count, uint64_t* branch_sig) {          \
         RasterIn<T> a{C, N, D, W, H, tile_size, tile_w, tile_h, n_isects, means2d, M, colors, opacities, normals,    \
                       textures, tex_ry, tex_rx, (T)range_x, (T)range_y, backgrounds, masks, offsets, flatten_ids,     \
-                      gaussian_ids, (T)contrib_threshold, (T)g_weight};                                              \
+                      gaussian_ids, (T)contrib_threshold, (T)g_weight, mip_L};                                       \
         RasterOut<T> o{out_colors, out_alphas, out_normals, out_distort, out_median, last_ids, median_ids,            \
                        contrib_sum, contrib_count};                                                                   \
         raster_fwd<T>(a, o, pair_count, branch_sig);                                                                             \
@@ -898,14 +960,14 @@ void sh_bwd(int64_t n, int degree, int K, const T* dirs, const T* coeffs, const 
     TGO_EXPORT void tgo_raster_bwd_##SUF(                                                                            \
         int C, int N, int D, int W, int H, int tile_size, int tile_w, int tile_h, int64_t n_isects, int64_t E,       \
         const T* means2d, const T* M, const T* colors, const T* opacities, const T* normals, const T* textures,       \
-        int tex_ry, int tex_rx, double range_x, double range_y, const T* backgrounds, const uint8_t* masks,           \
+        int tex_ry, int tex_rx, int mip_L, double range_x, double range_y, const T* backgrounds, const uint8_t* masks, \
         const int32_t* offsets, const int32_t* flatten_ids, const int64_t* gaussian_ids, double g_weight,             \
         const T* f_colors, const T* f_alphas, const int32_t* last_ids, const int32_t* median_ids, const T* v_colors,  \
         const T* v_alphas, const T* v_normals, const T* v_distort, const T* v_median, int mode, T* g_means2d,         \
         T* g_means2d_abs, T* g_M, T* g_colors, T* g_opacities, T* g_normals, T* g_textures, T* g_densify) {           \
         RasterIn<T> a{C, N, D, W, H, tile_size, tile_w, tile_h, n_isects, means2d, M, colors, opacities, normals,    \
                       textures, tex_ry, tex_rx, (T)range_x, (T)range_y, backgrounds, masks, offsets, flatten_ids,     \
-                      gaussian_ids, T(0), (T)g_weight};                                                              \
+                      gaussian_ids, T(0), (T)g_weight, mip_L};                                                       \
         RasterGradIn<T> gi{f_colors, f_alphas, last_ids, median_ids, v_colors, v_alphas, v_normals, v_distort,       \
                            v_median};                                                                                \
         RasterGradOut<T> go{g_means2d, g_means2d_abs, g_M, g_colors, g_opacities, g_normals, g_textures, g_densify}; \

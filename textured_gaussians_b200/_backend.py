@@ -79,7 +79,7 @@ class RasterFwdArgs(ctypes.Structure):
                 ("out_colors", P), ("out_alphas", P), ("out_normals", P), ("out_distort", P), ("out_median", P),
                 ("last_ids", P), ("median_ids", P), ("contrib_sum", P), ("contrib_count", P), ("tile_order", P),
                 ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64), ("n_isects_dev", P),
-                ("batch_depth", I32), ("work_queue", P)]
+                ("batch_depth", I32), ("work_queue", P), ("mip_levels", I32), ("tex_coarse", P)]
 
 
 class RasterBwdArgs(ctypes.Structure):
@@ -87,7 +87,7 @@ class RasterBwdArgs(ctypes.Structure):
                 ("median_ids", P), ("v_render_colors", P), ("v_render_alphas", P), ("v_render_normals", P),
                 ("v_render_distort", P), ("v_render_median", P), ("adjoint", I32), ("n_elems", I64),
                 ("v_means2d", P), ("v_means2d_abs", P), ("v_ray_transforms", P), ("v_colors", P),
-                ("v_opacities", P), ("v_normals", P), ("v_textures", P), ("v_densify", P)]
+                ("v_opacities", P), ("v_normals", P), ("v_textures", P), ("v_densify", P), ("v_tex_coarse", P)]
 
 
 _lib = None
@@ -126,6 +126,8 @@ def lib() -> ctypes.CDLL:
                 ("tg_sh_fwd", [I64, I64, I32, I32, P, P, P, P, P]),
                 ("tg_selective_adam", [P, P, P, P, P, F32, F32, F32, F32, I64, I64, I32, P, P]),
                 ("tg_densify_stats", [ctypes.POINTER(DensifyStatsArgs), P]),
+                ("tg_generate_mipmap", [P, P, I64, I32, P]),
+                ("tg_generate_mipmap_bwd", [P, P, I64, I32, P]),
                 ("tg_sh_bwd", [I64, I64, I32, I32, P, P, P, P, P, P, P]),
             ]:
                 fn = getattr(L, name)

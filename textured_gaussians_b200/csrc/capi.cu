@@ -44,6 +44,8 @@ cudaError_t launch_selective_adam(float* param, const float* grad, float* m, flo
                                   float b1, float b2, float eps, int64_t N, int64_t M, int shadow_format, void* shadow,
                                   cudaStream_t s);
 cudaError_t launch_densify_stats(const tg_densify_stats_args& a, cudaStream_t s);
+cudaError_t launch_generate_mipmap(const float* textures, float* coarse, int64_t G, int L, cudaStream_t s);
+cudaError_t launch_generate_mipmap_bwd(float* v_coarse, float* v_textures, int64_t G, int L, cudaStream_t s);
 int fail_with(int code, const char* msg);
 }  // namespace tg
 
@@ -143,6 +145,18 @@ int check_raster_common(const tg_raster_fwd_args& a) {
     if (a.tex_format != TG_TEX_NONE)
         TG_REQUIRE(a.tex_rx >= 1 && a.tex_ry >= 1 && a.range_x > 0.f && a.range_y > 0.f, TG_ERR_INVALID_ARG,
                    "bad texture size or range");
+    TG_REQUIRE(a.mip_levels >= 0 && a.mip_levels <= 15, TG_ERR_INVALID_ARG, "bad mip_levels %d", a.mip_levels);
+    if (a.mip_levels > 0) {
+        TG_REQUIRE(a.tex_format == TG_TEX_F32 || a.tex_format == TG_TEX_BF16, TG_ERR_UNSUPPORTED,
+                   "the mipmapped2 filter supports FP32 and BF16 texture storage");
+        TG_REQUIRE(a.D == 3 || a.D == 4, TG_ERR_UNSUPPORTED, "the mipmapped2 filter supports 3 or 4 channels");
+        TG_REQUIRE(a.tex_rx == (1 << a.mip_levels) && a.tex_ry == a.tex_rx, TG_ERR_INVALID_ARG,
+                   "mipmapped2 textures must be 2^L x 2^L (got %d x %d for L = %d)", a.tex_ry, a.tex_rx, a.mip_levels);
+        TG_REQUIRE(a.tex_coarse && aligned(a.tex_coarse, 16), TG_ERR_INVALID_ARG,
+                   "mipmapped2 needs the 16-byte aligned coarse pyramid");
+        TG_REQUIRE(a.tile_size <= 16 && a.work_queue == nullptr, TG_ERR_UNSUPPORTED,
+                   "the mipmapped2 filter runs with tile 8 or 16 and one CTA per tile");
+    }
     return TG_OK;
 }
 }  // namespace
@@ -396,6 +410,11 @@ int tg_rasterize_bwd(const tg_raster_bwd_args* a, tg_stream_t stream) {
     int rc = check_raster_common(a->f);
     if (rc != TG_OK) return rc;
     TG_REQUIRE(a->adjoint >= 0 && a->adjoint <= 2, TG_ERR_INVALID_ARG, "bad adjoint %d", a->adjoint);
+    TG_REQUIRE(a->f.mip_levels == 0 || a->adjoint == TG_ADJ_REFERENCE, TG_ERR_UNSUPPORTED,
+               "the mipmapped2 filter has the reference adjoint only");
+    if (a->f.mip_levels > 0 && a->v_textures)
+        TG_REQUIRE(a->v_tex_coarse && aligned(a->v_tex_coarse, 16), TG_ERR_INVALID_ARG,
+                   "mipmapped2 texture gradients need v_tex_coarse");
     TG_REQUIRE(a->n_elems >= 0, TG_ERR_INVALID_ARG, "negative n_elems");
     TG_REQUIRE(a->render_colors && a->render_alphas && a->last_ids && a->median_ids && a->v_render_colors &&
                    a->v_render_alphas && a->v_render_normals && a->v_render_distort && a->v_render_median,
@@ -412,7 +431,11 @@ int tg_rasterize_bwd(const tg_raster_bwd_args* a, tg_stream_t stream) {
         {a->v_means2d, sizeof(float) * 2 * E}, {a->v_ray_transforms, sizeof(float) * 9 * E},
         {a->v_colors, sizeof(float) * D * E},  {a->v_opacities, sizeof(float) * E},
         {a->v_normals, sizeof(float) * 3 * E}, {a->v_means2d_abs, a->v_means2d_abs ? sizeof(float) * 2 * E : 0},
-        {a->v_textures, tex_bytes},            {a->v_densify, sizeof(float) * 2 * E}};
+        {a->v_textures, tex_bytes},            {a->v_densify, sizeof(float) * 2 * E},
+        {a->v_tex_coarse, a->f.mip_levels > 0 && a->v_textures
+                              ? sizeof(float) * 4 * (size_t)(((int64_t(1) << (2 * a->f.mip_levels)) - 1) / 3) *
+                                    (size_t)a->f.n_contrib
+                              : 0}};
     for (const Z& z : zs)
         if (z.p && z.n) {
             cudaError_t e = cudaMemsetAsync(z.p, 0, z.n, stream);
@@ -455,6 +478,22 @@ int tg_selective_adam(float* param, const float* grad, float* exp_avg, float* ex
     return cuda_status(tg::launch_selective_adam(param, grad, exp_avg, exp_avg_sq, visibility, lr, b1, b2, eps, N, M,
                                                  shadow_format, shadow, stream),
                        "tg_selective_adam");
+}
+
+int tg_generate_mipmap(const float* textures, float* coarse, int64_t G, int32_t L, tg_stream_t stream) {
+    TG_REQUIRE(G >= 0 && L >= 1 && L <= 15, TG_ERR_INVALID_ARG, "bad sizes (G %lld, L %d)", (long long)G, L);
+    if (G == 0) return TG_OK;
+    TG_REQUIRE(textures && coarse && aligned(textures, 16) && aligned(coarse, 16), TG_ERR_INVALID_ARG,
+               "null or misaligned pointer");
+    return cuda_status(tg::launch_generate_mipmap(textures, coarse, G, L, stream), "tg_generate_mipmap");
+}
+
+int tg_generate_mipmap_bwd(float* v_coarse, float* v_textures, int64_t G, int32_t L, tg_stream_t stream) {
+    TG_REQUIRE(G >= 0 && L >= 1 && L <= 15, TG_ERR_INVALID_ARG, "bad sizes (G %lld, L %d)", (long long)G, L);
+    if (G == 0) return TG_OK;
+    TG_REQUIRE(v_coarse && v_textures && aligned(v_coarse, 16) && aligned(v_textures, 16), TG_ERR_INVALID_ARG,
+               "null or misaligned pointer");
+    return cuda_status(tg::launch_generate_mipmap_bwd(v_coarse, v_textures, G, L, stream), "tg_generate_mipmap_bwd");
 }
 
 int tg_densify_stats(const tg_densify_stats_args* a, tg_stream_t stream) {

@@ -82,10 +82,11 @@ struct PixelAdj {
 // sums `vals` (slots of GradSlots<D>), issues the pair's texel-gradient atomics,
 // and advances the pixel's back-to-front state.  Follows
 // rasterize_to_pixels_textured_gaussians_2dgs_bwd.cu:438-627 (+ bwd2.cu:612-676).
-template <int D, class Tex>
-__device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, const PairEval& e, PixelAdj<D>& P,
-                                                const float4 xyo, const float4 nn, const float* cp, int32_t idx,
-                                                float* vt, float uv_scale, float (&vals)[32]) {
+template <int D, class Tex, class Filt = FiltBilinear>
+__device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, const PairEvalT<Filt::kTaps>& e,
+                                                PixelAdj<D>& P, const float4 xyo, const float4 nn, const float* cp,
+                                                int32_t idx, float* vt, float uv_scale, float (&vals)[32],
+                                                float* vct = nullptr, int mip_clen = 0) {
     constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
     using GS = GradSlots<D>;
     const tg_raster_fwd_args& f = a.f;
@@ -145,17 +146,24 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
     }
     if (kTextured && e.tex_valid && vt != nullptr) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < Filt::kTaps; ++q) {
             float4 gq;
             gq.x = 0 < D ? fac * e.w[q] * P.v_c[0] : 0.f;
             gq.y = 1 < D ? fac * e.w[q] * P.v_c[1 < D ? 1 : 0] : 0.f;
             gq.z = 2 < D ? fac * e.w[q] * P.v_c[2 < D ? 2 : 0] : 0.f;
             gq.w = (3 < D ? fac * e.w[q] * P.v_c[3 < D ? 3 : 0] : 0.f) + e.w[q] * tex_a_grad;
-            if (gq.x != 0.f || gq.y != 0.f || gq.z != 0.f || gq.w != 0.f)
-                atomicAdd(reinterpret_cast<float4*>(vt + 4 * (int64_t)e.toff[q]), gq);
+            if (gq.x != 0.f || gq.y != 0.f || gq.z != 0.f || gq.w != 0.f) {
+                if constexpr (Filt::kMip) {  // pyramid coordinate: coarse levels, or level 0 = the texture
+                    const int mc = e.toff[q];
+                    float* dst = mc < mip_clen ? vct + 4 * (int64_t)mc : vt + 4 * (int64_t)(mc - mip_clen);
+                    atomicAdd(reinterpret_cast<float4*>(dst), gq);
+                } else {
+                    atomicAdd(reinterpret_cast<float4*>(vt + 4 * (int64_t)e.toff[q]), gq);
+                }
+            }
         }
     }
-    if (kTextured && e.tex_valid && uv_scale != 0.f) {
+    if (!Filt::kMip && kTextured && e.tex_valid && uv_scale != 0.f) {
         const float wu = e.w[1] + e.w[3], wv = e.w[2] + e.w[3];
         const float dbu[4] = {-(1.f - wv), 1.f - wv, -wv, wv};
         const float dbv[4] = {-(1.f - wu), -wu, 1.f - wu, wu};
@@ -199,7 +207,7 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
 }
 
 // One work item (tile) of the adjoint; every early return is uniform over the CTA.
-template <int D, class Tex, int PPT>
+template <int D, class Tex, int PPT, class Filt = FiltBilinear>
 __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const float uv_scale, const int bs,
                                          const int64_t item) {
     using GS = GradSlots<D>;
@@ -297,6 +305,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
     __syncthreads();
     const int32_t block_max_bin = s_max_bin;
     const int64_t tex_stride = (int64_t)f.tex_ry * f.tex_rx;
+    const int mip_clen = Filt::kMip ? ((1 << (2 * f.mip_levels)) - 1) / 3 : 0;
 
     for (int32_t batch_end = range_end - 1; batch_end >= range_start; batch_end -= bs) {
         if (batch_end - (bs - 1) > block_max_bin) continue;  // every splat here is past all last contributors
@@ -335,6 +344,8 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
             const float4 nn = s_nrm[t];
             const float* cp = s_col + t * D;
             float* vt = a.v_textures != nullptr ? a.v_textures + 4 * tex_base : nullptr;
+            float* vct = Filt::kMip && a.v_tex_coarse != nullptr ? a.v_tex_coarse + 4 * (int64_t)row * mip_clen
+                                                                 : nullptr;
             float vals[32];
 #pragma unroll
             for (int k = 0; k < 32; ++k) vals[k] = 0.f;
@@ -342,12 +353,13 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
 #pragma unroll
             for (int q = 0; q < PPT; ++q) {
                 if (!(P[q].inside && idx <= P[q].bin_final) || !in_box(box, P[q].px, P[q].py)) continue;
-                PairEval e;
-                eval_pair<Tex>(e, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx, f.tex_ry,
-                               f.range_x, f.range_y, f.g_weight);
+                PairEvalT<Filt::kTaps> e;
+                eval_pair<Tex, Filt>(e, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx,
+                                     f.tex_ry, f.range_x, f.range_y, f.g_weight,
+                                     MipSrc{f.tex_coarse, (int64_t)row * mip_clen, mip_clen, f.mip_levels});
                 if (!e.valid) continue;
                 any = true;
-                accumulate_pair<D, Tex>(a, e, P[q], xyo, nn, cp, idx, vt, uv_scale, vals);
+                accumulate_pair<D, Tex, Filt>(a, e, P[q], xyo, nn, cp, idx, vt, uv_scale, vals, vct, mip_clen);
             }
             if (!__any_sync(wmask, any)) continue;
             warp_reduce_scatter32(vals, wmask);
@@ -375,13 +387,13 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
 
 // CTA per work item, or (work_queue != NULL) a persistent grid whose CTAs take
 // items from the queue counter until none is left.
-template <int D, class Tex, int PPT, bool kPersistent>
+template <int D, class Tex, int PPT, bool kPersistent, class Filt = FiltBilinear>
 __global__ void __launch_bounds__(256, BwdBounds<PPT>::kMinCtas) raster_bwd_kernel(const tg_raster_bwd_args a,
                                                                                    const float uv_scale,
                                                                                    const int bs,
                                                                                    const int64_t n_items) {
     if constexpr (!kPersistent) {
-        bwd_tile<D, Tex, PPT>(a, uv_scale, bs, blockIdx.x);
+        bwd_tile<D, Tex, PPT, Filt>(a, uv_scale, bs, blockIdx.x);
         return;
     }
     else {
@@ -392,7 +404,7 @@ __global__ void __launch_bounds__(256, BwdBounds<PPT>::kMinCtas) raster_bwd_kern
             const int64_t item = s_item;
             __syncthreads();  // s_item read by all before it is rewritten
             if (item >= n_items) return;
-            bwd_tile<D, Tex, PPT>(a, uv_scale, bs, item);
+            bwd_tile<D, Tex, PPT, Filt>(a, uv_scale, bs, item);
         }
     }
 }
@@ -419,9 +431,15 @@ cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     const size_t smem = bwd_smem_bytes(D, bs);
     const int64_t blocks = f.views ? f.n_tiles : (int64_t)f.C * f.tile_width * f.tile_height;
     const float uv_scale = a.adjoint == TG_ADJ_BWD2 ? 1.f : (a.adjoint == TG_ADJ_EXACT ? 0.5f : 0.f);
+    bool mip = false;
+    if constexpr ((D == 3 || D == 4) && (Tex::kFormat == TG_TEX_F32 || Tex::kFormat == TG_TEX_BF16))
+        mip = f.mip_levels > 0;  // mipmapped2: one pixel per thread, one CTA per tile
+    else if (f.mip_levels > 0)
+        return cudaErrorInvalidValue;
     const bool four = tile_px > 256;  // 32x32 tiles: four pixels per thread, 256 threads
     const bool pers = f.work_queue != nullptr;
-    const void* fn = four ? (pers ? (const void*)raster_bwd_kernel<D, Tex, 4, true>
+    const void* fn = mip ? (const void*)raster_bwd_kernel<D, Tex, 1, false, FiltMip2>
+                   : four ? (pers ? (const void*)raster_bwd_kernel<D, Tex, 4, true>
                                   : (const void*)raster_bwd_kernel<D, Tex, 4, false>)
                           : (pers ? (const void*)raster_bwd_kernel<D, Tex, 1, true>
                                   : (const void*)raster_bwd_kernel<D, Tex, 1, false>);
@@ -435,7 +453,8 @@ cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
             if ((err = persistent_grid(fn, threads, smem, blocks, grid)) != cudaSuccess) return err;
         }
         const dim3 g((unsigned)grid), b((unsigned)threads);
-        if (four && pers) raster_bwd_kernel<D, Tex, 4, true><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        if (mip) raster_bwd_kernel<D, Tex, 1, false, FiltMip2><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        else if (four && pers) raster_bwd_kernel<D, Tex, 4, true><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
         else if (four) raster_bwd_kernel<D, Tex, 4, false><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
         else if (pers) raster_bwd_kernel<D, Tex, 1, true><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
         else raster_bwd_kernel<D, Tex, 1, false><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);

@@ -4,8 +4,9 @@
 // therefore the set of splats that contributed to a pixel -- is recomputed
 // bit-identically in the backward.  The arithmetic follows
 // rasterize_to_pixels_textured_gaussians_2dgs_fwd.cu:283-347 (textured) and
-// rasterize_to_pixels_2dgs_fwd.cu:281-310 (plain) of the reference, and the
-// bilinear addressing filters/bilinear.cuh:16-64.
+// rasterize_to_pixels_2dgs_fwd.cu:281-310 (plain) of the reference, the
+// bilinear addressing filters/bilinear.cuh:16-64, and for the mipmapped2
+// filter rasterize_to_pixels_mip2_textured_gaussians_2dgs_fwd.cu:293-347.
 #pragma once
 #include "tg_common.cuh"
 
@@ -13,22 +14,101 @@ namespace tg {
 
 constexpr float kFilterInvSquare = 2.0f;
 
-struct PairEval {
+// Texture filters: bilinear (4 taps in the splat's texture) and mipmapped2
+// (8 taps: bilinear in the two pyramid levels around the pixel footprint's
+// level, filters/mip2.cuh:27-105 of the reference).
+struct FiltBilinear {
+    static constexpr int kTaps = 4;
+    static constexpr bool kMip = false;
+};
+struct FiltMip2 {
+    static constexpr int kTaps = 8;
+    static constexpr bool kMip = true;
+};
+
+template <int NT>
+struct PairEvalT {
     f3 hu, hv, z;
     float sx, sy, dx, dy;
     float g3, g2, kern, vis, alpha, asf;
-    float w[4];
-    float4 tx[4];  // the four RGBA taps
-    int toff[4];   // texel index of each tap inside the splat's texture
+    float w[NT];
+    float4 tx[NT];  // the RGBA taps
+    int toff[NT];   // bilinear: texel index in the splat's texture; mip: pyramid coordinate (see MipSrc)
     bool valid, tex_valid;
 };
+using PairEval = PairEvalT<4>;
+
+// Coarse pyramid levels of the mip filter for one splat.  Pyramid coordinate
+// mc addresses the reference's per-splat pyramid [coarse levels | level 0]:
+// mc < clen lies in `coarse` (levels 1..L, FP32), mc >= clen is texel mc - clen
+// of the splat's full-resolution texture (the texture storage itself, so level
+// 0 is never copied).
+struct MipSrc {
+    const float* coarse;
+    int64_t cbase;  // first coarse texel of the splat
+    int clen;       // coarse texels per splat: (4^L - 1) / 3
+    int L;          // log2 of the texture side
+};
+
+// First pyramid coordinate of level t (side 2^(L-t)): (4^(L-t) - 1) / 3.
+__device__ __forceinline__ int mip_level_base(int L, int t) { return ((1 << ((L - t) * 2)) - 1) / 3; }
+
+// Trilinear taps of the mipmapped2 filter (filters/mip2.cuh:27-105): level
+// t = log2 of the largest texture-space footprint edge, clamped to [0, 31],
+// bilinear taps in levels floor(t) and ceil(t) with corner-aligned coordinates
+// (u + 0.5) / 2^level - 0.5; false when a tap falls outside its level (also
+// for a level beyond the coarsest, where the reference's index is undefined).
+__device__ __forceinline__ bool mip2_taps(float sx, float sy, float dxx, float dxy, float dyx, float dyy, int R, int L,
+                                          float range_x, float range_y, int (&mc)[8], float (&w)[8]) {
+    const float fr = (float)(R - 1);
+    const float ax = dxx / (range_x * 2.f) * fr, ay = dxy / (range_x * 2.f) * fr;  // both with range_x, as the reference
+    const float bx = dyx / (range_y * 2.f) * fr, by = dyy / (range_y * 2.f) * fr;
+    const float duv = fmaxf(sqrtf(ax * ax + ay * ay), sqrtf(bx * bx + by * by));
+    float t = log2f(duv);
+    if (t < 0.f) t = 0.f;
+    else if (t > 31.f) t = 31.f;
+    const float u = (sx + range_x) / (range_x * 2.f) * fr;
+    const float v = (sy + range_y) / (range_y * 2.f) * fr;
+    const int tl = (int)floorf(t), th = (int)ceilf(t);
+    if (th > L) return false;
+    const float il = 1.f / (float)(1u << tl), ih = 1.f / (float)(1u << th);  // exact powers of two
+    const float us = (u + 0.5f) * il - 0.5f, ug = (u + 0.5f) * ih - 0.5f;
+    const float vs = (v + 0.5f) * il - 0.5f, vg = (v + 0.5f) * ih - 0.5f;
+    const int uls = (int)floorf(us), ulg = (int)floorf(ug), vls = (int)floorf(vs), vlg = (int)floorf(vg);
+    const int uhs = (int)ceilf(us), uhg = (int)ceilf(ug), vhs = (int)ceilf(vs), vhg = (int)ceilf(vg);
+    if (uls < 0 || ulg < 0 || vls < 0 || vlg < 0 || uhs > ((R - 1) >> tl) || uhg > ((R - 1) >> th) ||
+        vhs > ((R - 1) >> tl) || vhg > ((R - 1) >> th))
+        return false;
+    const int rl = R >> tl, rh = R >> th;
+    const int bl = mip_level_base(L, tl), bh = mip_level_base(L, th);
+    mc[0] = bl + vls * rl + uls;
+    mc[1] = bl + vls * rl + uhs;
+    mc[2] = bl + vhs * rl + uls;
+    mc[3] = bl + vhs * rl + uhs;
+    mc[4] = bh + vlg * rh + ulg;
+    mc[5] = bh + vlg * rh + uhg;
+    mc[6] = bh + vhg * rh + ulg;
+    mc[7] = bh + vhg * rh + uhg;
+    const float wus = us - (float)uls, wvs = vs - (float)vls, wug = ug - (float)ulg, wvg = vg - (float)vlg;
+    const float wt = t - (float)tl;
+    w[0] = (1.f - wus) * (1.f - wvs) * (1.f - wt);
+    w[1] = wus * (1.f - wvs) * (1.f - wt);
+    w[2] = (1.f - wus) * wvs * (1.f - wt);
+    w[3] = wus * wvs * (1.f - wt);
+    w[4] = (1.f - wug) * (1.f - wvg) * wt;
+    w[5] = wug * (1.f - wvg) * wt;
+    w[6] = (1.f - wug) * wvg * wt;
+    w[7] = wug * wvg * wt;
+    return true;
+}
 
 // Splat data staged in shared memory: xyo = (x, y, opacity, texture scale),
 // m0/m1/m2 = rows of the ray transform (w unused).
-template <class Tex>
-__device__ __forceinline__ void eval_pair(PairEval& e, float px, float py, const float4 xyo, const float4 m0,
-                                          const float4 m1, const float4 m2, const void* textures, int64_t tex_base,
-                                          int rx, int ry, float range_x, float range_y, float g_weight) {
+template <class Tex, class Filt = FiltBilinear>
+__device__ __forceinline__ void eval_pair(PairEvalT<Filt::kTaps>& e, float px, float py, const float4 xyo,
+                                          const float4 m0, const float4 m1, const float4 m2, const void* textures,
+                                          int64_t tex_base, int rx, int ry, float range_x, float range_y,
+                                          float g_weight, const MipSrc mip = MipSrc{nullptr, 0, 0, 0}) {
     constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
     e.hu = mk3(px * m2.x - m0.x, px * m2.y - m0.y, px * m2.z - m0.z);
     e.hv = mk3(py * m2.x - m1.x, py * m2.y - m1.y, py * m2.z - m1.z);
@@ -43,7 +123,30 @@ __device__ __forceinline__ void eval_pair(PairEval& e, float px, float py, const
     const float iz = 1.f / e.z.z;
     e.sx = e.z.x * iz;
     e.sy = e.z.y * iz;
-    if (kTextured) {
+    if constexpr (Filt::kMip) {
+        // s at the pixel's left/right and top/bottom edge midpoints: the texture-space footprint
+        const f3 hw = mk3(0.5f * m2.x, 0.5f * m2.y, 0.5f * m2.z);
+        const f3 cx0 = cross(e.hu - hw, e.hv), cx1 = cross(e.hu + hw, e.hv);
+        const f3 cy0 = cross(e.hu, e.hv - hw), cy1 = cross(e.hu, e.hv + hw);
+        if (cx0.z == 0.f || cx1.z == 0.f || cy0.z == 0.f || cy1.z == 0.f) {
+            e.valid = false;
+            return;
+        }
+        const float dxx = cx1.x / cx1.z - cx0.x / cx0.z, dxy = cx1.y / cx1.z - cx0.y / cx0.z;
+        const float dyx = cy1.x / cy1.z - cy0.x / cy0.z, dyy = cy1.y / cy1.z - cy0.y / cy0.z;
+        if (mip2_taps(e.sx, e.sy, dxx, dxy, dyx, dyy, rx, mip.L, range_x, range_y, e.toff, e.w)) {
+            float asf = 0.f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int mc = e.toff[i];
+                e.tx[i] = mc < mip.clen ? __ldg(reinterpret_cast<const float4*>(mip.coarse) + mip.cbase + mc)
+                                        : Tex::load(textures, tex_base + (mc - mip.clen), xyo.w);
+                asf += e.w[i] * e.tx[i].w;
+            }
+            e.asf = asf;
+            e.tex_valid = true;
+        }
+    } else if (kTextured) {
         if (!(e.sx < -range_x || e.sx > range_x || e.sy < -range_y || e.sy > range_y)) {
             // u = (s + range) / (2 range) * (R - 1), clamped to [0, R-1]
             const float ku = (float)(rx - 1) / (range_x * 2.f), kv = (float)(ry - 1) / (range_y * 2.f);
@@ -149,11 +252,12 @@ __device__ __forceinline__ bool in_box(const float4 b, float px, float py) {
 }
 
 // Texture contribution to colour channel k (channels >= 4 have none).
-__device__ __forceinline__ float tex_color(const PairEval& e, int k) {
+template <int NT>
+__device__ __forceinline__ float tex_color(const PairEvalT<NT>& e, int k) {
     if (k >= 4 || !e.tex_valid) return 0.f;
     float s = 0.f;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) s += e.w[i] * f4get(e.tx[i], k);
+    for (int i = 0; i < NT; ++i) s += e.w[i] * f4get(e.tx[i], k);
     return s;
 }
 

@@ -35,7 +35,7 @@ struct FwdBounds {
 };
 
 // One work item (tile) of the forward; every early return is uniform over the CTA.
-template <int D, class Tex, int PPT>
+template <int D, class Tex, int PPT, class Filt = FiltBilinear>
 __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int bs, const int64_t item) {
     constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
     extern __shared__ float4 smem4[];
@@ -104,6 +104,7 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
     const int32_t range_end = tc.range_end;
     const int num_batches = (range_end - range_start + bs - 1) / bs;
     const int64_t tex_stride = (int64_t)a.tex_ry * a.tex_rx;
+    const int mip_clen = Filt::kMip ? ((1 << (2 * a.mip_levels)) - 1) / 3 : 0;
 
     float T[PPT], pix_out[PPT][D], nrm_out[PPT][3], distort[PPT], accum_vis_depth[PPT], median_depth[PPT];
     int32_t cur_idx[PPT], median_idx[PPT];
@@ -161,9 +162,10 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
 #pragma unroll
             for (int q = 0; q < PPT; ++q) {
                 if (done[q] || !in_box(box, px[q], py[q])) continue;
-                PairEval e;
-                eval_pair<Tex>(e, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx, a.tex_ry, a.range_x,
-                               a.range_y, a.g_weight);
+                PairEvalT<Filt::kTaps> e;
+                eval_pair<Tex, Filt>(e, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx, a.tex_ry,
+                                     a.range_x, a.range_y, a.g_weight,
+                                     MipSrc{a.tex_coarse, (int64_t)row * mip_clen, mip_clen, a.mip_levels});
                 if (!e.valid) continue;
                 const float next_T = T[q] * (1.f - e.alpha);
                 if (next_T <= 1e-4f) {
@@ -223,12 +225,12 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
 
 // CTA per work item, or (work_queue != NULL) a persistent grid whose CTAs take
 // items from the queue counter until none is left.
-template <int D, class Tex, int PPT, bool kPersistent>
+template <int D, class Tex, int PPT, bool kPersistent, class Filt = FiltBilinear>
 __global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kernel(const tg_raster_fwd_args a,
                                                                                    const int bs,
                                                                                    const int64_t n_items) {
     if constexpr (!kPersistent) {
-        fwd_tile<D, Tex, PPT>(a, bs, blockIdx.x);
+        fwd_tile<D, Tex, PPT, Filt>(a, bs, blockIdx.x);
         return;
     }
     else {
@@ -239,15 +241,35 @@ __global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kern
             const int64_t item = s_item;
             __syncthreads();  // s_item read by all before it is rewritten
             if (item >= n_items) return;
-            fwd_tile<D, Tex, PPT>(a, bs, item);
+            fwd_tile<D, Tex, PPT, Filt>(a, bs, item);
         }
     }
 }
 
 size_t fwd_smem_bytes(int D, int bs) { return (size_t)bs * (6 * sizeof(float4) + D * sizeof(float) + sizeof(int)); }
 
+// mipmapped2 filter: one pixel per thread (8x8 / 16x16 tiles), one CTA per tile
+template <int D, class Tex>
+cudaError_t launch_fwd_mip(const tg_raster_fwd_args& a, cudaStream_t s) {
+    const int tile_px = a.tile_size * a.tile_size;
+    const int bs = a.batch_depth > 0 ? a.batch_depth : tile_px;
+    const size_t smem = fwd_smem_bytes(D, bs);
+    const int64_t blocks = a.views ? a.n_tiles : (int64_t)a.C * a.tile_width * a.tile_height;
+    if (blocks == 0) return cudaSuccess;
+    cudaError_t err = cudaFuncSetAttribute(raster_fwd_kernel<D, Tex, 1, false, FiltMip2>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    raster_fwd_kernel<D, Tex, 1, false, FiltMip2><<<(unsigned)blocks, tile_px, smem, s>>>(a, bs, blocks);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
 template <int D, class Tex>
 cudaError_t launch_fwd_t(const tg_raster_fwd_args& a, cudaStream_t s) {
+    if constexpr ((D == 3 || D == 4) && (Tex::kFormat == TG_TEX_F32 || Tex::kFormat == TG_TEX_BF16)) {
+        if (a.mip_levels > 0) return launch_fwd_mip<D, Tex>(a, s);
+    }
+    if (a.mip_levels > 0) return cudaErrorInvalidValue;
     const int tile_px = a.tile_size * a.tile_size;
     const int bs = a.batch_depth > 0 ? a.batch_depth : tile_px;
     const size_t smem = fwd_smem_bytes(D, bs);

@@ -36,7 +36,9 @@ _FILTER_ADJOINT = {
     "bilinear": B.TG_ADJ_REFERENCE,
     "bilinear_bwd2": B.TG_ADJ_BWD2,
     "bilinear_exact": B.TG_ADJ_EXACT,
+    "mipmapped2": B.TG_ADJ_REFERENCE,
 }
+_MIP_FILTERS = ("mipmapped2",)
 
 
 def _bit_width(n: int) -> int:
@@ -559,9 +561,60 @@ def make_texture_storage(textures: Tensor, fmt: str) -> Tuple[Tensor, Optional[T
     raise ValueError(f"unknown texture storage format {fmt!r}")
 
 
+def mip_levels_of(textures: Tensor) -> int:
+    """L of square 2^L x 2^L textures [G, R, R, 4] (the mipmapped2 filter's requirement, reference
+    cuda/_wrapper.py:1946-1950)."""
+    R = int(textures.shape[1])
+    L = R.bit_length() - 1
+    if textures.dim() != 4 or textures.shape[2] != R or R != 1 << L or L < 1:
+        raise ValueError(f"mipmapped2 needs square power-of-two textures of side >= 2, got {tuple(textures.shape)}")
+    return L
+
+
+def _coarse_pyramid(textures: Tensor, L: int) -> Tensor:
+    """Levels 1..L of the textures' mip pyramid, [G, (4^L - 1) / 3, 4] FP32, coarsest first."""
+    src = textures.detach().float().contiguous()
+    G = src.shape[0]
+    coarse = torch.empty((G, (4 ** L - 1) // 3, 4), dtype=torch.float32, device=src.device)
+    st = B.stream_of(src)
+    B.call("tg_generate_mipmap", st, B.lib().tg_generate_mipmap, B.ptr(src), B.ptr(coarse), G, L, st)
+    return coarse
+
+
+class _GenerateMipmap(torch.autograd.Function):
+    """Full mip pyramid [G, (4^(L+1) - 1) / 3, 4] of 2^L textures in the reference's layout (coarse levels, then
+    level 0), mirroring _GenerateMipmap (reference cuda/_wrapper.py:4015-4058)."""
+
+    @staticmethod
+    def forward(ctx, textures, L):
+        G, R = textures.shape[0], textures.shape[1]
+        coarse = _coarse_pyramid(textures, L)
+        ctx.L, ctx.shape = L, textures.shape
+        return torch.cat([coarse, textures.detach().float().reshape(G, R * R, -1)], dim=1)
+
+    @staticmethod
+    def backward(ctx, v_mip):
+        L = ctx.L
+        G, R = ctx.shape[0], ctx.shape[1]
+        clen = (4 ** L - 1) // 3
+        v_mip = v_mip.float()
+        v_coarse = v_mip[:, :clen].contiguous().clone()
+        v_tex = v_mip[:, clen:].reshape(G, R, R, -1).contiguous().clone()
+        st = B.stream_of(v_tex)
+        B.call("tg_generate_mipmap_bwd", st, B.lib().tg_generate_mipmap_bwd, B.ptr(v_coarse), B.ptr(v_tex), G, L, st)
+        return v_tex, None
+
+
+def generate_mipmap(textures: Tensor, log_texture_res: int, log_reduce: int = 4, tile_size: int = 16) -> Tensor:
+    """Mip pyramid of 2^L textures (reference ``generate_mipmap``, cuda/_wrapper.py:4052-4058).  ``log_reduce`` and
+    ``tile_size`` only set the reference's launch shape and are accepted for compatibility."""
+    assert textures.shape[1] == textures.shape[2] == 1 << log_texture_res, textures.shape
+    return _GenerateMipmap.apply(textures, int(log_texture_res))
+
+
 def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_store, tex_scales, range_x, range_y,
               backgrounds, masks, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-              gs_contrib_threshold, g_weight, C, N, layout=None, n_isects_dev=None):
+              gs_contrib_threshold, g_weight, C, N, layout=None, n_isects_dev=None, mip_levels=0, tex_coarse=None):
     D = colors.shape[-1]
     vt = None if layout is None else layout.get("view_table")
     th, tw = (1, 1) if vt is not None else isect_offsets.shape[1:3]
@@ -581,7 +634,7 @@ def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_stor
         None if vt is None else B.ptr(vt.views), None if vt is None else B.ptr(vt.tile_view),
         0 if vt is None else vt.n_tiles, 0 if vt is None else vt.n_pixels, B.ptr(n_isects_dev),
         0 if layout is None else layout.get("batch_depth", 0),
-        None if layout is None else B.ptr(layout.get("work_queue")))
+        None if layout is None else B.ptr(layout.get("work_queue")), int(mip_levels), B.ptr(tex_coarse))
 
 
 class _RasterizeToPixelsTextured(torch.autograd.Function):
@@ -590,13 +643,19 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
     Mirrors _RasterizeToPixelsTexturedGaussians (reference cuda/_wrapper.py:2947-3155)
     and _RasterizeToPixels2DGS (:2767-2944): saves the inputs plus the final
     colours, alphas, last and median ids -- no per-splat transmittance.
+    With ``mip_levels`` L > 0 (the mipmapped2 filter, reference
+    _RasterizeToPixelsMip2TexturedGaussians) the forward builds the coarse
+    levels of the FP32 textures, and the backward folds their gradient into
+    the texture gradient in place (no full-pyramid tensor in either pass).
     """
 
     @staticmethod
     def forward(ctx, means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, masks,
                 tex_store, tex_scales, range_x, range_y, width, height, tile_size, isect_offsets, flatten_ids,
-                absgrad, gs_contrib_threshold, g_weight, adjoint, bg_grad_index_ok, gaussian_ids, n_rows, layout):
+                absgrad, gs_contrib_threshold, g_weight, adjoint, bg_grad_index_ok, gaussian_ids, n_rows, layout,
+                mip_levels=0):
         dev = means2d.device
+        coarse = _coarse_pyramid(textures, mip_levels) if mip_levels else None
         vt = None if layout is None else layout.get("view_table")
         C = isect_offsets.shape[0] if vt is None else vt.n_views
         # per-pixel output shape: [C, H, W] for one image size, [n_pixels] over the flat views
@@ -609,7 +668,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         n_dev = getattr(flatten_ids, "_tg_n_isects", None)
         a = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
                       backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-                      gs_contrib_threshold, g_weight, C, N, layout, n_dev)
+                      gs_contrib_threshold, g_weight, C, N, layout, n_dev, mip_levels, coarse)
         render_colors = torch.empty(pshape + (D,), dtype=torch.float32, device=dev)
         render_alphas = torch.empty(pshape + (1,), dtype=torch.float32, device=dev)
         render_normals = torch.empty(pshape + (3,), dtype=torch.float32, device=dev)
@@ -632,6 +691,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
                    gs_contrib_threshold, N, n_contrib, C, pshape)
         ctx.layout = layout
         ctx.n_isects_dev = n_dev
+        ctx.mip = (mip_levels, coarse)
         ctx.mark_non_differentiable(contrib_sum, contrib_count)
         return render_colors, render_alphas, render_normals, render_distort, render_median, contrib_sum, contrib_count
 
@@ -656,7 +716,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         v_rm = g(v_render_median, pshape + (1,))
         f = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
                       backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-                      0.0, g_weight, C, N, ctx.layout, ctx.n_isects_dev)
+                      0.0, g_weight, C, N, ctx.layout, ctx.n_isects_dev, *ctx.mip)
         v_means2d = torch.empty_like(means2d)
         v_means2d_abs = torch.empty_like(means2d) if absgrad else None
         v_ray_transforms = torch.empty_like(ray_transforms)
@@ -671,8 +731,14 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
                             means2d.numel() // 2, B.ptr(v_means2d), B.ptr(v_means2d_abs),
                             B.ptr(v_ray_transforms), B.ptr(v_colors), B.ptr(v_opacities), B.ptr(v_normals),
                             B.ptr(v_textures), B.ptr(v_densify))
+        L = ctx.mip[0]
+        v_coarse = torch.empty_like(ctx.mip[1]) if L and want_tex else None
+        a.v_tex_coarse = B.ptr(v_coarse)
         st = B.stream_of(means2d)
         B.call("tg_rasterize_bwd", st, B.lib().tg_rasterize_bwd, ctypes.byref(a), st)
+        if v_coarse is not None:
+            B.call("tg_generate_mipmap_bwd", st, B.lib().tg_generate_mipmap_bwd, B.ptr(v_coarse), B.ptr(v_textures),
+                   textures.shape[0], L, st)
         if absgrad:
             means2d.absgrad = v_means2d_abs
         v_backgrounds = None
@@ -687,7 +753,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
             v_textures = v_textures.to(textures.dtype)
         return (v_means2d, v_ray_transforms, v_colors, v_opacities, v_textures, v_normals, v_densify, v_backgrounds,
                 None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None,
-                None)
+                None, None)
 
 
 def _layout(tile_order, view_table, batch_depth=0, persistent=False, device=None):
@@ -787,6 +853,7 @@ def rasterize_to_pixels_textured_gaussians(
     if filtering not in _FILTER_ADJOINT:
         raise Exception(f"Unsupported filter type {filtering}")
     assert textures.dim() == 4 and textures.shape[-1] == 4, textures.shape
+    mip_levels = mip_levels_of(textures) if filtering in _MIP_FILTERS else 0
     if packed:
         if gaussian_ids is None:
             raise ValueError("packed textured rasterization needs gaussian_ids (texture row of each packed entry)")
@@ -809,7 +876,7 @@ def rasterize_to_pixels_textured_gaussians(
         float(texture_range_x), float(texture_range_y), int(image_width), int(image_height), int(tile_size),
         isect_offsets.contiguous(), flatten_ids.contiguous(), absgrad, gs_contrib_threshold, g_weight,
         _FILTER_ADJOINT[filtering], False, gaussian_ids, textures.shape[0],
-        _layout(tile_order, view_table, batch_depth, persistent, means2d.device))
+        _layout(tile_order, view_table, batch_depth, persistent, means2d.device), mip_levels)
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]
