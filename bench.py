@@ -252,7 +252,7 @@ def _run_ours(args, rank, world, local, dev):
     w_rgb = torch.randn((C, H, W, 3), generator=g, device=dev)
     w_a = torch.randn((C, H, W, 1), generator=g, device=dev)
 
-    def step(storage, tile_size, per_view, depth=0, persistent=False):
+    def step(storage, tile_size, per_view, depth=0, persistent=False, filtering="bilinear"):
         for t in (means, quats, scales, opac, colors, tex32):
             t.grad = None
         views = [slice(c, c + 1) for c in range(C)] if per_view else [slice(0, C)]
@@ -261,14 +261,14 @@ def _run_ours(args, rank, world, local, dev):
                                                    sh_degree=0, far_plane=100.0, tile_size=tile_size,
                                                    texture_storage=storage,
                                                    tile_order=args.tile_order, batch_depth=depth,
-                                                   persistent=persistent)
+                                                   persistent=persistent, filtering=filtering)
             loss = (out[0] * w_rgb[v]).sum() + (out[1] * w_a[v]).sum()
             loss.backward()
         return out, loss
 
-    def timed(storage, tile_size, per_view, steps, warmup, depth=0):
+    def timed(storage, tile_size, per_view, steps, warmup, depth=0, filtering="bilinear"):
         for _ in range(warmup):
-            step(storage, tile_size, per_view, depth)
+            step(storage, tile_size, per_view, depth, filtering=filtering)
         torch.cuda.synchronize()
         barrier(world)
         torch.cuda.synchronize()
@@ -282,7 +282,7 @@ def _run_ours(args, rank, world, local, dev):
             t0.record()
             for i in range(steps):
                 starts[i].record()
-                out, _ = step(storage, tile_size, per_view, depth)
+                out, _ = step(storage, tile_size, per_view, depth, filtering=filtering)
                 ends[i].record()
             t1.record()
             torch.cuda.synchronize()
@@ -320,6 +320,20 @@ def _run_ours(args, rank, world, local, dev):
     # FP32 plain drop-in on the same GPU: FP32 textures, one camera per call, tile 16
     total_f32, per_f32, stages_f32, launches_f32, _ = timed(None, 16, True, args.steps, args.warmup)
     total_f32 = max_over_ranks(total_f32, world)
+    # the same headline form with the other texture filters: mipmapped2 (coarse levels built and folded back
+    # every step) and anisotropic_bilinear (each pixel's footprint integrated over the texel cells it covers)
+    filters = {}
+    if not args.no_filters:
+        f_tile = min(tile, 16)
+        for filt in ("mipmapped2", "anisotropic_bilinear"):
+            total_f, _, stages_f, _, out_f = timed(store, f_tile, False, args.steps, args.warmup,
+                                                   depth if f_tile == tile else 0, filt)
+            del out_f
+            total_f = max_over_ranks(total_f, world)
+            filters[filt] = {
+                "value": round(C * H * W * world * args.steps / (total_f / 1e3) / 1e6, 2), "unit": "Mpix/s",
+                "ms_per_step": round(total_f / args.steps, 3), "tile_size": f_tile,
+                "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stages_f.items()}}
 
     pix_per_step = C * H * W * world
     value = pix_per_step * args.steps / (total_bf16 / 1e3) / 1e6
@@ -363,7 +377,7 @@ def _run_ours(args, rank, world, local, dev):
                        "stage_ms": stage_ms_f32},
         "bf16_over_fp32": round(value / value_f32, 3),
         "stage_ms": stage_ms, "per_step_ms": [round(x, 3) for x in per_bf16],
-        "graphed": graphed, "persistent_ms_per_step": round(pers_ms, 3),
+        "graphed": graphed, "persistent_ms_per_step": round(pers_ms, 3), "filters": filters,
         "counts": counts, "roofline": roofline, "gpu_launches": int(launches),
         "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cpu,
     }
@@ -714,6 +728,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay timing")
+    ap.add_argument("--no-filters", action="store_true", help="skip the other texture filters' timing")
     ap.add_argument("--workload", default="mixture1m", choices=["mixture1m", "batch"],
                     help="mixture1m: the headline workload; batch: 64 uneven views over 3 scenes (batching form)")
     ap.add_argument("--views", type=int, default=64, help="views of the batch workload")

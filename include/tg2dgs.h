@@ -47,6 +47,12 @@ typedef struct CUstream_st* tg_stream_t; /* same type as cudaStream_t */
 #define TG_ADJ_BWD2 1      /* "bilinear_bwd2": reference UV term (du/ds factor (R-1)/range) */
 #define TG_ADJ_EXACT 2     /* exact derivative of the forward ((R-1)/(2*range)) */
 
+/* Texture filters of the compositor (tg_raster_fwd_args.filter).  mipmapped2
+ * is selected by mip_levels > 0 (filter 0 or TG_FILTER_MIPMAPPED2). */
+#define TG_FILTER_BILINEAR 0
+#define TG_FILTER_MIPMAPPED2 1
+#define TG_FILTER_ANISO_BILINEAR 2
+
 /* ------------------------------------------------------------------ batching form
  * Views of uneven size in one call (no counterpart in the reference, which
  * renders C cameras of one size per call).  A batch of C views is described by
@@ -371,7 +377,7 @@ typedef struct {
      * it until none is left.  NULL: one CTA per work item. */
     uint32_t* work_queue;
     /* The mipmapped2 filter (mip_levels = L > 0; rasterize_to_pixels_mip2_
-     * textured_gaussians_2dgs_fwd.cu of the reference): textures are 2^L x 2^L
+     * textured_gaussians_2dgs_fwd.cu of the reference): textures are 2^L x 2^L (L <= 13)
      * (tex_ry = tex_rx = 2^L) and tex_coarse holds their coarser levels,
      * [G, (4^L - 1) / 3, 4] FP32 in the reference's pyramid order (coarsest
      * first, as made by tg_generate_mipmap); level 0 is read from `textures`.
@@ -379,6 +385,13 @@ typedef struct {
      * persistent launch, and the reference adjoint. */
     int32_t mip_levels;
     const float* tex_coarse;
+    /* TG_FILTER_ANISO_BILINEAR: the anisotropic_bilinear filter
+     * (rasterize_to_pixels_aniso_bilinear_textured_gaussians_2dgs_{fwd,bwd}.cu
+     * of the reference): each pixel's footprint quad in texel space integrates
+     * the bilinear interpolant cell by cell.  Same support as mipmapped2
+     * (F32 / BF16 storage, 3 or 4 channels, tile 8 or 16, one CTA per tile,
+     * reference adjoint). */
+    int32_t filter;
 } tg_raster_fwd_args;
 TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
 
@@ -436,7 +449,8 @@ TG_API int tg_sh_bwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, c
  * The reference also copies level 0 into its pyramid; here the compositor
  * reads level 0 from the texture storage itself.  The adjoint adds each coarse
  * gradient / 4 into its four children, coarsest to finest, ending in
- * v_textures (accumulated, not overwritten); v_coarse is modified in place. */
+ * v_textures (accumulated, not overwritten); v_coarse is scratch (levels 5,
+ * 10, ... are modified when L > 5).  1 <= L <= 13. */
 TG_API int tg_generate_mipmap(const float* textures, float* coarse, int64_t G, int32_t L, tg_stream_t stream);
 TG_API int tg_generate_mipmap_bwd(float* v_coarse, float* v_textures, int64_t G, int32_t L, tg_stream_t stream);
 

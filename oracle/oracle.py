@@ -47,14 +47,16 @@ def lib():
             getattr(_LIB, f"tgo_sh_fwd_{suf}").argtypes = [c_i64, c_int, c_int] + [c_ptr] * 4
             getattr(_LIB, f"tgo_sh_bwd_{suf}").argtypes = [c_i64, c_int, c_int] + [c_ptr] * 6
             getattr(_LIB, f"tgo_raster_fwd_{suf}").argtypes = (
-                [c_int] * 8 + [c_i64] + [c_ptr] * 6 + [c_int, c_int, c_int, c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl, c_dbl]
+                [c_int] * 8 + [c_i64] + [c_ptr] * 6 + [c_int] * 4 + [c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl, c_dbl]
                 + [c_ptr] * 11
             )
             getattr(_LIB, f"tgo_raster_bwd_{suf}").argtypes = (
-                [c_int] * 8 + [c_i64, c_i64] + [c_ptr] * 6 + [c_int, c_int, c_int, c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl]
+                [c_int] * 8 + [c_i64, c_i64] + [c_ptr] * 6 + [c_int] * 4 + [c_dbl, c_dbl] + [c_ptr] * 5 + [c_dbl]
                 + [c_ptr] * 9 + [c_int] + [c_ptr] * 8
             )
         _LIB.tgo_sort_pairs.argtypes = [c_i64, c_ptr, c_ptr, c_int]
+        _LIB.tgo_aniso_sample.argtypes = [c_ptr, c_int, c_int, c_ptr, c_ptr]
+        _LIB.tgo_aniso_sample.restype = c_dbl
         _LIB.tgo_offset_encode.argtypes = [c_i64, c_ptr, c_int, c_int, c_int, c_ptr]
     return _LIB
 
@@ -209,6 +211,17 @@ def _tex_shape(textures, mip_levels):
     return textures.shape[1], textures.shape[2]
 
 
+def aniso_sample(corners, texture):
+    """anisotropic_bilinear filter of one footprint quad (corners [4,2] in texel coordinates) over a texture
+    [ry, rx, 4], in FP64: the bilinear interpolant integrated over the quad's part inside the texel grid,
+    divided by the quad's area.  Returns (rgba [4], area)."""
+    c = np.ascontiguousarray(corners, np.float64).reshape(4, 2)
+    t = np.ascontiguousarray(texture, np.float64)
+    out = np.zeros(4, np.float64)
+    area = lib().tgo_aniso_sample(_p(c), t.shape[1], t.shape[0], _p(t), _p(out))
+    return out, area
+
+
 def mip_level_base(L: int, t: int) -> int:
     """Texel index of level t (side 2^(L-t)) in the pyramid of a 2^L texture, coarsest first (filters/mip2.cuh:15-25)."""
     return (4 ** (L - t) - 1) // 3
@@ -250,13 +263,14 @@ def generate_mipmap_bwd(v_pyramid, L: int):
 
 def raster_fwd(means2d, M, colors, opacities, normals, textures, offsets, flatten_ids, W, H, tile_size,
                range_x=3.0, range_y=3.0, backgrounds=None, masks=None, gaussian_ids=None, n_gauss=None,
-               contrib_threshold=0.0, g_weight=1.0, mip_levels=0, dtype=np.float32):
+               contrib_threshold=0.0, g_weight=1.0, mip_levels=0, aniso=False, dtype=np.float32):
     """Compositor forward.  ``textures=None`` selects the plain 2DGS compositor.
 
     Dense layout: means2d [C,N,2] ...; packed layout: [nnz,...] plus
     ``gaussian_ids`` [nnz] and ``n_gauss``.  ``mip_levels`` L > 0 selects the
     mipmapped2 filter on a 2^L x 2^L texture: ``textures`` is then the full
-    pyramid [G, (4^(L+1)-1)/3, 4] of :func:`generate_mipmap`.
+    pyramid [G, (4^(L+1)-1)/3, 4] of :func:`generate_mipmap`.  ``aniso``
+    selects the anisotropic_bilinear filter (footprint-integrated bilinear).
     """
     means2d, M, colors, opacities, normals, textures, backgrounds = (
         _c(x, dtype) for x in (means2d, M, colors, opacities, normals, textures, backgrounds))
@@ -278,7 +292,7 @@ def raster_fwd(means2d, M, colors, opacities, normals, textures, offsets, flatte
         branch_sig=np.zeros((C, H, W), np.uint64))
     getattr(lib(), f"tgo_raster_fwd_{_suf(dtype)}")(
         C, N, D, int(W), int(H), tile_size, tw, th, flatten_ids.size, _p(means2d), _p(M), _p(colors), _p(opacities),
-        _p(normals), _p(textures), ry, rx, int(mip_levels), float(range_x), float(range_y), _p(backgrounds), _p(m),
+        _p(normals), _p(textures), ry, rx, int(mip_levels), int(bool(aniso)), float(range_x), float(range_y), _p(backgrounds), _p(m),
         _p(offsets), _p(flatten_ids), _p(gid), float(contrib_threshold), float(g_weight), _p(o.colors), _p(o.alphas),
         _p(o.normals), _p(o.distort), _p(o.median), _p(o.last_ids), _p(o.median_ids), _p(o.contrib_sum),
         _p(o.contrib_count), _p(o.pair_count), _p(o.branch_sig))
@@ -299,7 +313,8 @@ class RasterBwdOut:
 
 def raster_bwd(means2d, M, colors, opacities, normals, textures, offsets, flatten_ids, W, H, tile_size, fwd,
                v_colors, v_alphas, v_normals, v_distort, v_median, range_x=3.0, range_y=3.0, backgrounds=None,
-               masks=None, gaussian_ids=None, n_gauss=None, g_weight=1.0, mode=0, mip_levels=0, dtype=np.float32):
+               masks=None, gaussian_ids=None, n_gauss=None, g_weight=1.0, mode=0, mip_levels=0, aniso=False,
+               dtype=np.float32):
     """Compositor adjoint.  mode 0: reference "bilinear", 1: "bilinear_bwd2", 2: exact.  With ``mip_levels`` > 0
     (mipmapped2, mode 0 only, as the reference has no other) ``v_textures`` is the full pyramid's gradient."""
     means2d, M, colors, opacities, normals, textures, backgrounds = (
@@ -325,7 +340,7 @@ def raster_bwd(means2d, M, colors, opacities, normals, textures, offsets, flatte
         v_densify=np.zeros(means2d.shape, dtype))
     getattr(lib(), f"tgo_raster_bwd_{_suf(dtype)}")(
         C, N, D, int(W), int(H), tile_size, tw, th, flatten_ids.size, E, _p(means2d), _p(M), _p(colors),
-        _p(opacities), _p(normals), _p(textures), ry, rx, int(mip_levels), float(range_x), float(range_y), _p(backgrounds), _p(m),
+        _p(opacities), _p(normals), _p(textures), ry, rx, int(mip_levels), int(bool(aniso)), float(range_x), float(range_y), _p(backgrounds), _p(m),
         _p(offsets), _p(flatten_ids), _p(gid), float(g_weight), _p(fc), _p(fa), _p(li), _p(mi), _p(vc), _p(va),
         _p(vn), _p(vd), _p(vm), int(mode), _p(o.v_means2d), _p(o.v_means2d_abs), _p(o.v_M), _p(o.v_colors),
         _p(o.v_opacities), _p(o.v_normals), _p(o.v_textures), _p(o.v_densify))

@@ -373,6 +373,7 @@ template <typename T> struct RasterIn {
     const int64_t* gaussian_ids;  // packed: [nnz] texture row of each element, else null (row = e % N)
     T contrib_threshold, g_weight;
     int mip_L;  // 0: bilinear on [G,ry,rx,4]; L > 0: mipmapped2 on the full pyramid [G,(4^(L+1)-1)/3,4]
+    int aniso;  // 1: anisotropic_bilinear on [G,ry,rx,4]
 };
 
 template <typename T> inline int64_t tex_row(const RasterIn<T>& a, int64_t e) {
@@ -423,13 +424,134 @@ template <typename T> struct SplatEval {
     bool valid;
     int valid_tex;
     int uc[4], vc[4];  // bilinear texel coordinates
-    int nt;            // taps: 4 bilinear, 8 mipmapped2
-    int64_t ti[8];     // texel index of each tap within the splat's row
+    int nt;            // taps: 4 bilinear, 8 mipmapped2, 4 per footprint cell for anisotropic_bilinear
+    int64_t ti[8];     // texel index of each tap within the splat's row (fixed-size filters)
     T w[8];
+    bool dyn = false;  // anisotropic_bilinear: taps in ati / aw
+    std::vector<int64_t> ati;
+    std::vector<T> aw;
+    T area;  // anisotropic_bilinear: footprint area in texels
     T asf, g3, g2, kern, vis, alpha;
     V3<T> hu, hv, zeta;
     T sx, sy, dx, dy;
+    int64_t tap(int t) const { return dyn ? ati[t] : ti[t]; }
+    T wt(int t) const { return dyn ? aw[t] : w[t]; }
 };
+
+// ---------------------------------------------------------------- anisotropic_bilinear
+// Restates filters/anisotropic_bilinear.cuh:15-235: the pixel's footprint quad
+// in texel coordinates, clipped (Sutherland-Hodgman) against every texel cell
+// [u, u+1] x [v, v+1] it overlaps; the moments of each clipped polygon weight
+// the cell's four texels (the exact integral of the bilinear interpolant), and
+// the sum is divided by the quad's area.
+template <typename T> struct V2 { T x, y; };
+template <typename T> inline V2<T> v2sub(V2<T> a, V2<T> b) { return {a.x - b.x, a.y - b.y}; }
+template <typename T> inline T v2cross(V2<T> a, V2<T> b) { return a.x * b.y - a.y * b.x; }
+template <typename T> inline T v2dot(V2<T> a, V2<T> b) { return a.x * b.x + a.y * b.y; }
+
+// float -> int as the GPU converts: NaN -> 0, saturating at the int range
+template <typename T> inline int sat_int(T x) {
+    if (x != x) return 0;
+    if (x >= T(2147483647.0)) return 2147483647;
+    if (x <= T(-2147483648.0)) return -2147483647 - 1;
+    return (int)x;
+}
+
+template <typename T> struct AnisoFoot {
+    V2<T> s[4], n[4];
+    T nmax[4];
+    int minu, maxu, minv, maxv;
+};
+
+template <typename T> inline void aniso_edge_normal(V2<T> s0, V2<T> e, V2<T> c, V2<T>& n) {
+    if (e.x == 0 && e.y == 0) n = v2sub(s0, c);
+    else n = {e.y, -e.x};
+    const T l = std::sqrt(n.x * n.x + n.y * n.y);
+    if (l == 0) return;  // left as is (the reference ignores this status)
+    n.x /= l;
+    n.y /= l;
+}
+
+// Orientation, texel bounds, edge normals; returns the area (precompute, :193-245).
+template <typename T> inline T aniso_setup(AnisoFoot<T>& F, int rx, int ry) {
+    V2<T> e01 = v2sub(F.s[1], F.s[0]), e12 = v2sub(F.s[2], F.s[1]), e23 = v2sub(F.s[3], F.s[2]),
+          e30 = v2sub(F.s[0], F.s[3]);
+    T area = T(0.5) * (v2cross(e01, e12) + v2cross(e23, e30));
+    if (area < 0) {
+        area *= -1;
+        std::swap(F.s[1], F.s[3]);
+        e01 = v2sub(F.s[1], F.s[0]); e12 = v2sub(F.s[2], F.s[1]);
+        e23 = v2sub(F.s[3], F.s[2]); e30 = v2sub(F.s[0], F.s[3]);
+    }
+    const V2<T>* s = F.s;
+    F.minu = std::max(0, sat_int(std::floor(std::min(std::min(s[0].x, s[1].x), std::min(s[2].x, s[3].x)))));
+    F.maxu = std::min(rx - 1, sat_int(std::ceil(std::max(std::max(s[0].x, s[1].x), std::max(s[2].x, s[3].x)))));
+    F.minv = std::max(0, sat_int(std::floor(std::min(std::min(s[0].y, s[1].y), std::min(s[2].y, s[3].y)))));
+    F.maxv = std::min(ry - 1, sat_int(std::ceil(std::max(std::max(s[0].y, s[1].y), std::max(s[2].y, s[3].y)))));
+    const V2<T> c = {(((s[0].x + s[1].x) + s[2].x) + s[3].x) / T(4), (((s[0].y + s[1].y) + s[2].y) + s[3].y) / T(4)};
+    aniso_edge_normal(s[0], e01, c, F.n[0]);
+    aniso_edge_normal(s[1], e12, c, F.n[1]);
+    aniso_edge_normal(s[2], e23, c, F.n[2]);
+    aniso_edge_normal(s[3], e30, c, F.n[3]);
+    for (int i = 0; i < 4; ++i)
+        F.nmax[i] = std::max(std::abs(F.n[i].x * T(0.5) + F.n[i].y * T(0.5)),
+                             std::abs(F.n[i].x * T(0.5) + F.n[i].y * T(-0.5)));
+    return area;
+}
+
+// Moments (A, Sx, Sy, Sxy) of the quad clipped to cell (u, v), in cell-local
+// coordinates (clip_and_compute_moments, :58-190); false if fewer than 3
+// vertices remain.  A clip that would overflow 8 vertices (only a
+// self-intersecting quad can) also returns false.
+template <typename T> inline bool aniso_cell(const AnisoFoot<T>& F, int u, int v, T& A, T& Sx, T& Sy, T& Sxy) {
+    const V2<T> sc = {T(u) + T(0.5), T(v) + T(0.5)};
+    if (v2dot(v2sub(F.s[0], sc), F.n[0]) >= F.nmax[0] && v2dot(v2sub(F.s[1], sc), F.n[1]) >= F.nmax[1] &&
+        v2dot(v2sub(F.s[2], sc), F.n[2]) >= F.nmax[2] && v2dot(v2sub(F.s[3], sc), F.n[3]) >= F.nmax[3]) {
+        A = T(1); Sx = T(0.5); Sy = T(0.5); Sxy = T(0.25);
+        return true;
+    }
+    V2<T> p[8], q[8];
+    int n = 4;
+    for (int i = 0; i < 4; ++i) p[i] = {F.s[i].x - T(u), F.s[i].y - T(v)};
+    // one half-plane: axis 0 = x, 1 = y; keep coordinate >= 0 (hi = false) or <= 1 (hi = true)
+    auto clip = [&](const V2<T>* in, V2<T>* out, int axis, bool hi) -> int {
+        int m = 0;
+        for (int i = 0; i < n; ++i) {
+            const V2<T> a = in[i], b = in[(i + 1) % n];
+            const T ac = axis ? a.y : a.x, bc = axis ? b.y : b.x;
+            const bool ain = hi ? ac <= T(1) : ac >= T(0), bin = hi ? bc <= T(1) : bc >= T(0);
+            if (ain) {
+                if (m == 8) return -1;
+                out[m++] = a;
+            }
+            if (ain != bin) {
+                if (m == 8) return -1;
+                const T t = hi ? (ac - T(1)) / (ac - bc) : ac / (ac - bc);
+                out[m++] = axis ? V2<T>{a.x + t * (b.x - a.x), hi ? T(1) : T(0)}
+                                : V2<T>{hi ? T(1) : T(0), a.y + t * (b.y - a.y)};
+            }
+        }
+        return m;
+    };
+    if ((n = clip(p, q, 0, false)) < 3) return false;
+    if ((n = clip(q, p, 0, true)) < 3) return false;
+    if ((n = clip(p, q, 1, false)) < 3) return false;
+    if ((n = clip(q, p, 1, true)) < 3) return false;
+    A = Sx = Sy = Sxy = T(0);
+    for (int i = 0; i < n; ++i) {
+        const V2<T> a = p[i], b = p[(i + 1) % n];
+        const T c = v2cross(a, b);
+        A += c;
+        Sx += c * (a.x + b.x);
+        Sy += c * (a.y + b.y);
+        Sxy += c * (T(2) * a.x * a.y + a.x * b.y + b.x * a.y + T(2) * b.x * b.y);
+    }
+    A *= T(0.5);
+    Sx *= T(1) / T(6);
+    Sy *= T(1) / T(6);
+    Sxy *= T(1) / T(24);
+    return true;
+}
 
 // Per (pixel, splat) evaluation shared by forward and backward, as the
 // reference recomputes it (fwd.cu:283-347, bwd.cu:338-397).
@@ -447,7 +569,41 @@ inline void eval_splat(const RasterIn<T>& a, int64_t g, T px, T py, SplatEval<T>
     e.sx = e.zeta.x / e.zeta.z;
     e.sy = e.zeta.y / e.zeta.z;
     const T opac = a.opacities[g];
-    if (a.textures && a.mip_L > 0) {
+    if (a.textures && a.aniso) {
+        // anisotropic_bilinear (aniso_bilinear fwd.cu:296-340): s at the pixel's four corners
+        const V3<T> dxw = cross3(e.hu, M2), dyw = cross3(e.hv, M2);
+        const V3<T> hx = T(0.5) * dxw, hy = T(0.5) * dyw;
+        const V3<T> cr[4] = {(e.zeta - hx) - hy, (e.zeta + hx) - hy, (e.zeta + hx) + hy, (e.zeta - hx) + hy};
+        if (cr[0].z == T(0) || cr[1].z == T(0) || cr[2].z == T(0) || cr[3].z == T(0)) {
+            e.valid = false;
+            e.g3 = e.g2 = T(0);
+            return;
+        }
+        AnisoFoot<T> F;
+        for (int i = 0; i < 4; ++i)
+            F.s[i] = {(cr[i].x / cr[i].z + a.range_x) / (a.range_x * 2) * T(a.tex_rx - 1),
+                      (cr[i].y / cr[i].z + a.range_y) / (a.range_y * 2) * T(a.tex_ry - 1)};
+        e.area = aniso_setup(F, a.tex_rx, a.tex_ry);
+        e.dyn = true;
+        e.nt = 0;
+        e.valid_tex = (e.area == T(0) || F.minu == F.maxu || F.minv == F.maxv) ? 0 : 1;
+        if (e.valid_tex > 0) {
+            const T ia = T(1) / e.area;
+            for (int v = F.minv; v < F.maxv; ++v)
+                for (int u = F.minu; u < F.maxu; ++u) {
+                    T A, Sx, Sy, Sxy;
+                    if (!aniso_cell(F, u, v, A, Sx, Sy, Sxy)) continue;
+                    const int64_t t00 = (int64_t)v * a.tex_rx + u;
+                    const int64_t tq[4] = {t00, t00 + 1, t00 + a.tex_rx, t00 + a.tex_rx + 1};
+                    const T wq[4] = {((A - Sx) - Sy) + Sxy, Sx - Sxy, Sy - Sxy, Sxy};
+                    for (int q = 0; q < 4; ++q) {
+                        e.ati.push_back(tq[q]);
+                        e.aw.push_back(wq[q] * ia);
+                    }
+                }
+            e.nt = (int)e.ati.size();
+        }
+    } else if (a.textures && a.mip_L > 0) {
         // mipmapped2 (mip2 fwd.cu:293-347): s at the pixel's edge midpoints gives the footprint
         const V3<T> hw = T(0.5) * M2;
         const V3<T> cx0 = cross3(e.hu - hw, e.hv), cx1 = cross3(e.hu + hw, e.hv);
@@ -473,9 +629,9 @@ inline void eval_splat(const RasterIn<T>& a, int64_t g, T px, T py, SplatEval<T>
         if (e.valid_tex > 0) {
             const T* tex = a.textures + tex_row(a, g) * tex_texels(a) * 4;
             e.asf = 0;
-            for (int i = 0; i < e.nt; ++i) e.asf += e.w[i] * tex[e.ti[i] * 4 + 3];
+            for (int i = 0; i < e.nt; ++i) e.asf += e.wt(i) * tex[e.tap(i) * 4 + 3];
         } else {
-            e.asf = 1;
+            e.asf = a.aniso ? T(0) : T(1);  // anisotropic_bilinear zeroes alpha without a texture sample
         }
     } else {
         e.asf = 1;
@@ -494,6 +650,9 @@ inline void eval_splat(const RasterIn<T>& a, int64_t g, T px, T py, SplatEval<T>
         e.alpha = std::min(T(0.999), opac * e.vis);
     }
     if (sigma < T(0) || e.alpha < T(1) / T(255)) e.valid = false;
+    // anisotropic_bilinear tests the untextured alpha first (aniso_bilinear fwd.cu:358-366); the adjoint follows
+    // the forward's tests, so the pairs it revisits are the ones the forward composited
+    if (a.textures && a.aniso && opac * e.vis < T(1) / T(255)) e.valid = false;
 }
 
 template <typename T> inline T tex_channel(const RasterIn<T>& a, int64_t g, const SplatEval<T>& e, int k) {
@@ -501,7 +660,7 @@ template <typename T> inline T tex_channel(const RasterIn<T>& a, int64_t g, cons
     if (k >= 4 || e.valid_tex <= 0) return T(0);
     const T* tex = a.textures + tex_row(a, g) * tex_texels(a) * 4;
     T s = 0;
-    for (int i = 0; i < e.nt; ++i) s += e.w[i] * tex[e.ti[i] * 4 + k];
+    for (int i = 0; i < e.nt; ++i) s += e.wt(i) * tex[e.tap(i) * 4 + k];
     return s;
 }
 
@@ -568,7 +727,7 @@ void raster_fwd(const RasterIn<T>& a, const RasterOut<T>& o, int32_t* pair_count
                             mix(e.g3 <= e.g2 ? 3 : 4);
                             mix((uint64_t)(e.valid_tex + 2));
                             if (e.valid_tex > 0)
-                                for (int q = 0; q < e.nt; ++q) mix((uint64_t)e.ti[q]);
+                                for (int q = 0; q < e.nt; ++q) mix((uint64_t)e.tap(q));
                             const T op = a.opacities[g];
                             mix(a.textures ? (op * e.vis * e.asf <= T(0.999) ? 5 : 6) : (op * e.vis <= T(0.999) ? 5 : 6));
                         }
@@ -691,10 +850,13 @@ void raster_bwd(const RasterIn<T>& a, const RasterGradIn<T>& gi, const RasterGra
                         texc[k] = 0;
                         if (tex_on && k < 4)
                             for (int t = 0; t < e.nt; ++t) {
-                                const int64_t o = e.ti[t] * 4 + k;
-                                atomic_add(vtex + o, fac * e.w[t] * vc[k]);
-                                texc[k] += e.w[t] * tex[o];
+                                const int64_t o = e.tap(t) * 4 + k;
+                                atomic_add(vtex + o, fac * e.wt(t) * vc[k]);
+                                texc[k] += e.wt(t) * tex[o];
                             }
+                        // anisotropic_bilinear's adjoint uses the texture colour without the division by the
+                        // footprint area (aniso_bilinear bwd.cu:499-522 with filters/anisotropic_bilinear.cuh:372-389)
+                        if (a.aniso) texc[k] *= e.area;
                     }
                     T v_alpha = 0;
                     for (int k = 0; k < D; ++k) v_alpha += ((texc[k] + cp[k]) * Tr - buf[k] * ra) * vc[k];
@@ -740,9 +902,9 @@ void raster_bwd(const RasterIn<T>& a, const RasterGradIn<T>& gi, const RasterGra
                         }
                         v_op = a.textures ? e.vis * v_alpha * e.asf : e.vis * v_alpha;
                         if (tex_on)
-                            for (int t = 0; t < e.nt; ++t) atomic_add(vtex + e.ti[t] * 4 + 3, e.w[t] * e.vis * opac * v_alpha);
+                            for (int t = 0; t < e.nt; ++t) atomic_add(vtex + e.tap(t) * 4 + 3, e.wt(t) * e.vis * opac * v_alpha);
                     }
-                    if (mode >= 1 && tex_on && a.mip_L == 0) {
+                    if (mode >= 1 && tex_on && a.mip_L == 0 && !a.aniso) {
                         const T wu = e.w[1] + e.w[3], wv = e.w[2] + e.w[3];
                         const T dbu[4] = {-(T(1) - wv), T(1) - wv, -wv, wv};
                         const T dbv[4] = {-(T(1) - wu), -wu, T(1) - wu, wu};
@@ -946,13 +1108,14 @@ void sh_bwd(int64_t n, int degree, int K, const T* dirs, const T* coeffs, const 
     TGO_EXPORT void tgo_raster_fwd_##SUF(                                                                            \
         int C, int N, int D, int W, int H, int tile_size, int tile_w, int tile_h, int64_t n_isects, const T* means2d, \
         const T* M, const T* colors, const T* opacities, const T* normals, const T* textures, int tex_ry, int tex_rx, \
-        int mip_L, double range_x, double range_y, const T* backgrounds, const uint8_t* masks, const int32_t* offsets, \
+        int mip_L, int aniso, double range_x, double range_y, const T* backgrounds, const uint8_t* masks,             \
+        const int32_t* offsets,                                                                                      \
         const int32_t* flatten_ids, const int64_t* gaussian_ids, double contrib_threshold, double g_weight,           \
         T* out_colors, T* out_alphas, T* out_normals, T* out_distort, T* out_median, int32_t* last_ids,              \
         int32_t* median_ids, T* contrib_sum, T* contrib_count, int32_t* pair_count, uint64_t* branch_sig) {          \
         RasterIn<T> a{C, N, D, W, H, tile_size, tile_w, tile_h, n_isects, means2d, M, colors, opacities, normals,    \
                       textures, tex_ry, tex_rx, (T)range_x, (T)range_y, backgrounds, masks, offsets, flatten_ids,     \
-                      gaussian_ids, (T)contrib_threshold, (T)g_weight, mip_L};                                       \
+                      gaussian_ids, (T)contrib_threshold, (T)g_weight, mip_L, aniso};                                \
         RasterOut<T> o{out_colors, out_alphas, out_normals, out_distort, out_median, last_ids, median_ids,            \
                        contrib_sum, contrib_count};                                                                   \
         raster_fwd<T>(a, o, pair_count, branch_sig);                                                                             \
@@ -960,14 +1123,15 @@ void sh_bwd(int64_t n, int degree, int K, const T* dirs, const T* coeffs, const 
     TGO_EXPORT void tgo_raster_bwd_##SUF(                                                                            \
         int C, int N, int D, int W, int H, int tile_size, int tile_w, int tile_h, int64_t n_isects, int64_t E,       \
         const T* means2d, const T* M, const T* colors, const T* opacities, const T* normals, const T* textures,       \
-        int tex_ry, int tex_rx, int mip_L, double range_x, double range_y, const T* backgrounds, const uint8_t* masks, \
+        int tex_ry, int tex_rx, int mip_L, int aniso, double range_x, double range_y, const T* backgrounds,          \
+        const uint8_t* masks,                                                                                        \
         const int32_t* offsets, const int32_t* flatten_ids, const int64_t* gaussian_ids, double g_weight,             \
         const T* f_colors, const T* f_alphas, const int32_t* last_ids, const int32_t* median_ids, const T* v_colors,  \
         const T* v_alphas, const T* v_normals, const T* v_distort, const T* v_median, int mode, T* g_means2d,         \
         T* g_means2d_abs, T* g_M, T* g_colors, T* g_opacities, T* g_normals, T* g_textures, T* g_densify) {           \
         RasterIn<T> a{C, N, D, W, H, tile_size, tile_w, tile_h, n_isects, means2d, M, colors, opacities, normals,    \
                       textures, tex_ry, tex_rx, (T)range_x, (T)range_y, backgrounds, masks, offsets, flatten_ids,     \
-                      gaussian_ids, T(0), (T)g_weight, mip_L};                                                       \
+                      gaussian_ids, T(0), (T)g_weight, mip_L, aniso};                                                \
         RasterGradIn<T> gi{f_colors, f_alphas, last_ids, median_ids, v_colors, v_alphas, v_normals, v_distort,       \
                            v_median};                                                                                \
         RasterGradOut<T> go{g_means2d, g_means2d_abs, g_M, g_colors, g_opacities, g_normals, g_textures, g_densify}; \
@@ -976,6 +1140,27 @@ void sh_bwd(int64_t n, int degree, int K, const T* dirs, const T* coeffs, const 
 
 TGO_DEF_PROJ(f32, float)
 TGO_DEF_PROJ(f64, double)
+
+// anisotropic_bilinear on one footprint: corners [4,2] in texel coordinates, texture [ry,rx,4];
+// out = the filtered RGBA (zero when the footprint has no texture sample); returns the footprint area.
+TGO_EXPORT double tgo_aniso_sample(const double* corners, int rx, int ry, const double* tex, double* out) {
+    AnisoFoot<double> F;
+    for (int i = 0; i < 4; ++i) F.s[i] = {corners[2 * i], corners[2 * i + 1]};
+    const double area = aniso_setup(F, rx, ry);
+    for (int k = 0; k < 4; ++k) out[k] = 0;
+    if (area == 0 || F.minu == F.maxu || F.minv == F.maxv) return area;
+    for (int v = F.minv; v < F.maxv; ++v)
+        for (int u = F.minu; u < F.maxu; ++u) {
+            double A, Sx, Sy, Sxy;
+            if (!aniso_cell(F, u, v, A, Sx, Sy, Sxy)) continue;
+            const double w[4] = {((A - Sx) - Sy) + Sxy, Sx - Sxy, Sy - Sxy, Sxy};
+            const int64_t t00 = (int64_t)v * rx + u;
+            const int64_t tq[4] = {t00, t00 + 1, t00 + rx, t00 + rx + 1};
+            for (int q = 0; q < 4; ++q)
+                for (int k = 0; k < 4; ++k) out[k] += w[q] * tex[tq[q] * 4 + k] / area;
+        }
+    return area;
+}
 
 TGO_EXPORT void tgo_sort_pairs(int64_t n, int64_t* keys, int32_t* vals, int end_bit) { sort_pairs(n, keys, vals, end_bit); }
 

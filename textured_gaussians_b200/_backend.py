@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(_HERE, "libtg2dgs.so")
 
 TG_TEX_NONE, TG_TEX_F32, TG_TEX_BF16, TG_TEX_F16, TG_TEX_FP8_E4M3 = 0, 1, 2, 3, 4
 TG_ADJ_REFERENCE, TG_ADJ_BWD2, TG_ADJ_EXACT = 0, 1, 2
+TG_FILTER_BILINEAR, TG_FILTER_MIPMAPPED2, TG_FILTER_ANISO_BILINEAR = 0, 1, 2
 _ERRORS = {-1: "invalid argument", -2: "unsupported", -3: "CUDA error", -4: "workspace too small",
            -5: "device wait timed out"}
 
@@ -79,7 +80,8 @@ class RasterFwdArgs(ctypes.Structure):
                 ("out_colors", P), ("out_alphas", P), ("out_normals", P), ("out_distort", P), ("out_median", P),
                 ("last_ids", P), ("median_ids", P), ("contrib_sum", P), ("contrib_count", P), ("tile_order", P),
                 ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64), ("n_isects_dev", P),
-                ("batch_depth", I32), ("work_queue", P), ("mip_levels", I32), ("tex_coarse", P)]
+                ("batch_depth", I32), ("work_queue", P), ("mip_levels", I32), ("tex_coarse", P),
+                ("filter", I32)]
 
 
 class RasterBwdArgs(ctypes.Structure):

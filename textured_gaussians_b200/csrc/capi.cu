@@ -145,7 +145,7 @@ int check_raster_common(const tg_raster_fwd_args& a) {
     if (a.tex_format != TG_TEX_NONE)
         TG_REQUIRE(a.tex_rx >= 1 && a.tex_ry >= 1 && a.range_x > 0.f && a.range_y > 0.f, TG_ERR_INVALID_ARG,
                    "bad texture size or range");
-    TG_REQUIRE(a.mip_levels >= 0 && a.mip_levels <= 15, TG_ERR_INVALID_ARG, "bad mip_levels %d", a.mip_levels);
+    TG_REQUIRE(a.mip_levels >= 0 && a.mip_levels <= 13, TG_ERR_INVALID_ARG, "bad mip_levels %d", a.mip_levels);
     if (a.mip_levels > 0) {
         TG_REQUIRE(a.tex_format == TG_TEX_F32 || a.tex_format == TG_TEX_BF16, TG_ERR_UNSUPPORTED,
                    "the mipmapped2 filter supports FP32 and BF16 texture storage");
@@ -156,6 +156,18 @@ int check_raster_common(const tg_raster_fwd_args& a) {
                    "mipmapped2 needs the 16-byte aligned coarse pyramid");
         TG_REQUIRE(a.tile_size <= 16 && a.work_queue == nullptr, TG_ERR_UNSUPPORTED,
                    "the mipmapped2 filter runs with tile 8 or 16 and one CTA per tile");
+    }
+    TG_REQUIRE(a.filter == TG_FILTER_BILINEAR || a.filter == TG_FILTER_MIPMAPPED2 ||
+                   a.filter == TG_FILTER_ANISO_BILINEAR, TG_ERR_INVALID_ARG, "unknown filter %d", a.filter);
+    TG_REQUIRE(a.filter != TG_FILTER_MIPMAPPED2 || a.mip_levels > 0, TG_ERR_INVALID_ARG,
+               "TG_FILTER_MIPMAPPED2 needs mip_levels > 0");
+    if (a.filter == TG_FILTER_ANISO_BILINEAR) {
+        TG_REQUIRE(a.mip_levels == 0, TG_ERR_INVALID_ARG, "anisotropic_bilinear takes no mip levels");
+        TG_REQUIRE(a.tex_format == TG_TEX_F32 || a.tex_format == TG_TEX_BF16, TG_ERR_UNSUPPORTED,
+                   "the anisotropic_bilinear filter supports FP32 and BF16 texture storage");
+        TG_REQUIRE(a.D == 3 || a.D == 4, TG_ERR_UNSUPPORTED, "the anisotropic_bilinear filter supports 3 or 4 channels");
+        TG_REQUIRE(a.tile_size <= 16 && a.work_queue == nullptr, TG_ERR_UNSUPPORTED,
+                   "the anisotropic_bilinear filter runs with tile 8 or 16 and one CTA per tile");
     }
     return TG_OK;
 }
@@ -412,6 +424,8 @@ int tg_rasterize_bwd(const tg_raster_bwd_args* a, tg_stream_t stream) {
     TG_REQUIRE(a->adjoint >= 0 && a->adjoint <= 2, TG_ERR_INVALID_ARG, "bad adjoint %d", a->adjoint);
     TG_REQUIRE(a->f.mip_levels == 0 || a->adjoint == TG_ADJ_REFERENCE, TG_ERR_UNSUPPORTED,
                "the mipmapped2 filter has the reference adjoint only");
+    TG_REQUIRE(a->f.filter != TG_FILTER_ANISO_BILINEAR || a->adjoint == TG_ADJ_REFERENCE, TG_ERR_UNSUPPORTED,
+               "the anisotropic_bilinear filter has the reference adjoint only");
     if (a->f.mip_levels > 0 && a->v_textures)
         TG_REQUIRE(a->v_tex_coarse && aligned(a->v_tex_coarse, 16), TG_ERR_INVALID_ARG,
                    "mipmapped2 texture gradients need v_tex_coarse");
@@ -481,7 +495,7 @@ int tg_selective_adam(float* param, const float* grad, float* exp_avg, float* ex
 }
 
 int tg_generate_mipmap(const float* textures, float* coarse, int64_t G, int32_t L, tg_stream_t stream) {
-    TG_REQUIRE(G >= 0 && L >= 1 && L <= 15, TG_ERR_INVALID_ARG, "bad sizes (G %lld, L %d)", (long long)G, L);
+    TG_REQUIRE(G >= 0 && L >= 1 && L <= 13, TG_ERR_INVALID_ARG, "bad sizes (G %lld, L %d)", (long long)G, L);
     if (G == 0) return TG_OK;
     TG_REQUIRE(textures && coarse && aligned(textures, 16) && aligned(coarse, 16), TG_ERR_INVALID_ARG,
                "null or misaligned pointer");
@@ -489,7 +503,7 @@ int tg_generate_mipmap(const float* textures, float* coarse, int64_t G, int32_t 
 }
 
 int tg_generate_mipmap_bwd(float* v_coarse, float* v_textures, int64_t G, int32_t L, tg_stream_t stream) {
-    TG_REQUIRE(G >= 0 && L >= 1 && L <= 15, TG_ERR_INVALID_ARG, "bad sizes (G %lld, L %d)", (long long)G, L);
+    TG_REQUIRE(G >= 0 && L >= 1 && L <= 13, TG_ERR_INVALID_ARG, "bad sizes (G %lld, L %d)", (long long)G, L);
     if (G == 0) return TG_OK;
     TG_REQUIRE(v_coarse && v_textures && aligned(v_coarse, 16) && aligned(v_textures, 16), TG_ERR_INVALID_ARG,
                "null or misaligned pointer");

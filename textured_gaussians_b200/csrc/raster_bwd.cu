@@ -83,7 +83,7 @@ struct PixelAdj {
 // and advances the pixel's back-to-front state.  Follows
 // rasterize_to_pixels_textured_gaussians_2dgs_bwd.cu:438-627 (+ bwd2.cu:612-676).
 template <int D, class Tex, class Filt = FiltBilinear>
-__device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, const PairEvalT<Filt::kTaps>& e,
+__device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, const PairOf<Filt>& e,
                                                 PixelAdj<D>& P, const float4 xyo, const float4 nn, const float* cp,
                                                 int32_t idx, float* vt, float uv_scale, float (&vals)[32],
                                                 float* vct = nullptr, int mip_clen = 0) {
@@ -100,7 +100,7 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
 #pragma unroll
     for (int k = 0; k < D; ++k) {
         vals[GS::kRgb + k] += fac * P.v_c[k];
-        texc[k] = kTextured ? tex_color(e, k) : 0.f;
+        texc[k] = kTextured ? tex_color_adj(e, k) : 0.f;
     }
     float v_alpha = 0.f;
 #pragma unroll
@@ -144,7 +144,16 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
         vals[GS::kOpac] += kTextured ? e.vis * v_alpha * e.asf : e.vis * v_alpha;
         tex_a_grad = e.vis * opac * v_alpha;
     }
-    if (kTextured && e.tex_valid && vt != nullptr) {
+    if constexpr (Filt::kAniso) {
+        if (e.tex_valid && vt != nullptr) {
+            const float4 g = make_float4(D > 0 ? fac * P.v_c[0] : 0.f, D > 1 ? fac * P.v_c[D > 1 ? 1 : 0] : 0.f,
+                                         D > 2 ? fac * P.v_c[D > 2 ? 2 : 0] : 0.f,
+                                         (D > 3 ? fac * P.v_c[D > 3 ? 3 : 0] : 0.f) + tex_a_grad);
+            const float ia = e.F.iarea;
+            if (g.x != 0.f || g.y != 0.f || g.z != 0.f || g.w != 0.f)
+                aniso_scatter(e.F, vt, f.tex_rx, make_float4(g.x * ia, g.y * ia, g.z * ia, g.w * ia));
+        }
+    } else if (kTextured && e.tex_valid && vt != nullptr) {
 #pragma unroll
         for (int q = 0; q < Filt::kTaps; ++q) {
             float4 gq;
@@ -163,7 +172,7 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
             }
         }
     }
-    if (!Filt::kMip && kTextured && e.tex_valid && uv_scale != 0.f) {
+    if (!Filt::kMip && !Filt::kAniso && kTextured && e.tex_valid && uv_scale != 0.f) {
         const float wu = e.w[1] + e.w[3], wv = e.w[2] + e.w[3];
         const float dbu[4] = {-(1.f - wv), 1.f - wv, -wv, wv};
         const float dbv[4] = {-(1.f - wu), -wu, 1.f - wu, wu};
@@ -324,7 +333,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
                 s_m1[slot] = make_float4(m[3], m[4], m[5], 0.f);
                 s_m2[slot] = make_float4(m[6], m[7], m[8], 0.f);
                 s_box[slot] = cull_box(s_xyo[slot], s_m0[slot], s_m1[slot], s_m2[slot], Tex::kFormat != TG_TEX_NONE,
-                                       f.range_x, f.range_y, f.g_weight);
+                                       f.range_x, f.range_y, f.g_weight, !Filt::kAniso);
                 const float* n = f.normals + 3 * (int64_t)g;
                 s_nrm[slot] = make_float4(n[0], n[1], n[2], 0.f);
 #pragma unroll
@@ -353,7 +362,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
 #pragma unroll
             for (int q = 0; q < PPT; ++q) {
                 if (!(P[q].inside && idx <= P[q].bin_final) || !in_box(box, P[q].px, P[q].py)) continue;
-                PairEvalT<Filt::kTaps> e;
+                PairOf<Filt> e;
                 eval_pair<Tex, Filt>(e, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx,
                                      f.tex_ry, f.range_x, f.range_y, f.g_weight,
                                      MipSrc{f.tex_coarse, (int64_t)row * mip_clen, mip_clen, f.mip_levels});
@@ -423,6 +432,23 @@ size_t bwd_smem_bytes(int D, int bs) {
     return (size_t)bs * (6 * sizeof(float4) + D * sizeof(float) + 2 * sizeof(int) + (D + 17) * sizeof(float));
 }
 
+// The mipmapped2 / anisotropic_bilinear kernels exist for FP32 / BF16 storage and 3 or 4 channels only.
+template <int D, class Tex, class Filt>
+constexpr bool filter_instance() {
+    return (D == 3 || D == 4) && (Tex::kFormat == TG_TEX_F32 || Tex::kFormat == TG_TEX_BF16);
+}
+template <int D, class Tex, class Filt>
+const void* filter_bwd_fn() {
+    if constexpr (filter_instance<D, Tex, Filt>()) return (const void*)raster_bwd_kernel<D, Tex, 1, false, Filt>;
+    else return nullptr;
+}
+template <int D, class Tex, class Filt>
+void launch_filter_bwd(dim3 g, dim3 b, size_t smem, cudaStream_t s, const tg_raster_bwd_args& a, float uv_scale, int bs,
+                       int64_t blocks) {
+    if constexpr (filter_instance<D, Tex, Filt>())
+        raster_bwd_kernel<D, Tex, 1, false, Filt><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+}
+
 template <int D, class Tex>
 cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     const tg_raster_fwd_args& f = a.f;
@@ -431,14 +457,13 @@ cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     const size_t smem = bwd_smem_bytes(D, bs);
     const int64_t blocks = f.views ? f.n_tiles : (int64_t)f.C * f.tile_width * f.tile_height;
     const float uv_scale = a.adjoint == TG_ADJ_BWD2 ? 1.f : (a.adjoint == TG_ADJ_EXACT ? 0.5f : 0.f);
-    bool mip = false;
-    if constexpr ((D == 3 || D == 4) && (Tex::kFormat == TG_TEX_F32 || Tex::kFormat == TG_TEX_BF16))
-        mip = f.mip_levels > 0;  // mipmapped2: one pixel per thread, one CTA per tile
-    else if (f.mip_levels > 0)
-        return cudaErrorInvalidValue;
+    // mipmapped2 / anisotropic_bilinear: one pixel per thread, one CTA per tile
+    const bool mip = f.mip_levels > 0, aniso = f.filter == TG_FILTER_ANISO_BILINEAR;
+    if ((mip || aniso) && !filter_instance<D, Tex, FiltMip2>()) return cudaErrorInvalidValue;
     const bool four = tile_px > 256;  // 32x32 tiles: four pixels per thread, 256 threads
     const bool pers = f.work_queue != nullptr;
-    const void* fn = mip ? (const void*)raster_bwd_kernel<D, Tex, 1, false, FiltMip2>
+    const void* fn = mip ? filter_bwd_fn<D, Tex, FiltMip2>()
+                   : aniso ? filter_bwd_fn<D, Tex, FiltAniso>()
                    : four ? (pers ? (const void*)raster_bwd_kernel<D, Tex, 4, true>
                                   : (const void*)raster_bwd_kernel<D, Tex, 4, false>)
                           : (pers ? (const void*)raster_bwd_kernel<D, Tex, 1, true>
@@ -453,7 +478,8 @@ cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
             if ((err = persistent_grid(fn, threads, smem, blocks, grid)) != cudaSuccess) return err;
         }
         const dim3 g((unsigned)grid), b((unsigned)threads);
-        if (mip) raster_bwd_kernel<D, Tex, 1, false, FiltMip2><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        if (mip) launch_filter_bwd<D, Tex, FiltMip2>(g, b, smem, s, a, uv_scale, bs, blocks);
+        else if (aniso) launch_filter_bwd<D, Tex, FiltAniso>(g, b, smem, s, a, uv_scale, bs, blocks);
         else if (four && pers) raster_bwd_kernel<D, Tex, 4, true><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
         else if (four) raster_bwd_kernel<D, Tex, 4, false><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
         else if (pers) raster_bwd_kernel<D, Tex, 1, true><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);

@@ -5,8 +5,10 @@
 // bit-identically in the backward.  The arithmetic follows
 // rasterize_to_pixels_textured_gaussians_2dgs_fwd.cu:283-347 (textured) and
 // rasterize_to_pixels_2dgs_fwd.cu:281-310 (plain) of the reference, the
-// bilinear addressing filters/bilinear.cuh:16-64, and for the mipmapped2
-// filter rasterize_to_pixels_mip2_textured_gaussians_2dgs_fwd.cu:293-347.
+// bilinear addressing filters/bilinear.cuh:16-64, for the mipmapped2 filter
+// rasterize_to_pixels_mip2_textured_gaussians_2dgs_fwd.cu:293-347, and for the
+// anisotropic_bilinear filter
+// rasterize_to_pixels_aniso_bilinear_textured_gaussians_2dgs_fwd.cu:296-391.
 #pragma once
 #include "tg_common.cuh"
 
@@ -14,16 +16,25 @@ namespace tg {
 
 constexpr float kFilterInvSquare = 2.0f;
 
-// Texture filters: bilinear (4 taps in the splat's texture) and mipmapped2
+// Texture filters: bilinear (4 taps in the splat's texture), mipmapped2
 // (8 taps: bilinear in the two pyramid levels around the pixel footprint's
-// level, filters/mip2.cuh:27-105 of the reference).
+// level, filters/mip2.cuh:27-105 of the reference) and anisotropic_bilinear
+// (the bilinear interpolant integrated over the pixel's footprint quad,
+// filters/anisotropic_bilinear.cuh:15-400: a variable number of texel cells).
 struct FiltBilinear {
     static constexpr int kTaps = 4;
     static constexpr bool kMip = false;
+    static constexpr bool kAniso = false;
 };
 struct FiltMip2 {
     static constexpr int kTaps = 8;
     static constexpr bool kMip = true;
+    static constexpr bool kAniso = false;
+};
+struct FiltAniso {
+    static constexpr int kTaps = 1;  // unused: the footprint replaces the tap list
+    static constexpr bool kMip = false;
+    static constexpr bool kAniso = true;
 };
 
 template <int NT>
@@ -37,6 +48,208 @@ struct PairEvalT {
     bool valid, tex_valid;
 };
 using PairEval = PairEvalT<4>;
+
+// The anisotropic_bilinear footprint of one (pixel, splat) pair: the pixel's
+// corners mapped to texel coordinates (counter-clockwise), their edges, the
+// reference's edge normals and fast-path margins, the texel-cell range and
+// 1 / area; tsum is the texture integral before the division by the area.
+struct AnisoFoot {
+    float2 s[4], e[4], n[4];
+    float nmax[4];
+    int minu, maxu, minv, maxv;
+    float iarea;
+    bool convex;  // the four corner rays meet the splat plane on one side (same sign of z)
+};
+struct PairEvalAniso : PairEvalT<1> {
+    AnisoFoot F;
+    float4 tsum;
+};
+template <class Filt> struct PairOfT { using type = PairEvalT<Filt::kTaps>; };
+template <> struct PairOfT<FiltAniso> { using type = PairEvalAniso; };
+template <class Filt> using PairOf = typename PairOfT<Filt>::type;
+
+__device__ __forceinline__ float cross2(float2 a, float2 b) { return a.x * b.y - a.y * b.x; }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// Orientation (counter-clockwise), texel-cell range, edge normals and margins
+// of the footprint quad; returns its area (precompute,
+// filters/anisotropic_bilinear.cuh:193-245).
+__device__ __forceinline__ float aniso_setup(AnisoFoot& F, int rx, int ry) {
+    float area = 0.5f * (cross2(sub2(F.s[1], F.s[0]), sub2(F.s[2], F.s[1])) +
+                         cross2(sub2(F.s[3], F.s[2]), sub2(F.s[0], F.s[3])));
+    if (area < 0.f) {
+        area = -area;
+        const float2 t = F.s[1];
+        F.s[1] = F.s[3];
+        F.s[3] = t;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) F.e[i] = sub2(F.s[(i + 1) & 3], F.s[i]);
+    // float -> int conversions saturate (NaN -> 0), so the cell range stays within the texture
+    F.minu = max(0, (int)floorf(fminf(fminf(F.s[0].x, F.s[1].x), fminf(F.s[2].x, F.s[3].x))));
+    F.maxu = min(rx - 1, (int)ceilf(fmaxf(fmaxf(F.s[0].x, F.s[1].x), fmaxf(F.s[2].x, F.s[3].x))));
+    F.minv = max(0, (int)floorf(fminf(fminf(F.s[0].y, F.s[1].y), fminf(F.s[2].y, F.s[3].y))));
+    F.maxv = min(ry - 1, (int)ceilf(fmaxf(fmaxf(F.s[0].y, F.s[1].y), fmaxf(F.s[2].y, F.s[3].y))));
+    const float cx = (((F.s[0].x + F.s[1].x) + F.s[2].x) + F.s[3].x) * 0.25f;
+    const float cy = (((F.s[0].y + F.s[1].y) + F.s[2].y) + F.s[3].y) * 0.25f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float2 n = (F.e[i].x == 0.f && F.e[i].y == 0.f) ? make_float2(F.s[i].x - cx, F.s[i].y - cy)
+                                                        : make_float2(F.e[i].y, -F.e[i].x);
+        const float l = sqrtf(n.x * n.x + n.y * n.y);
+        if (l != 0.f) n = make_float2(n.x / l, n.y / l);
+        F.n[i] = n;
+        F.nmax[i] = fmaxf(fabsf(n.x * 0.5f + n.y * 0.5f), fabsf(n.x * 0.5f - n.y * 0.5f));
+    }
+    return area;
+}
+
+// Green's-theorem terms of one directed boundary segment a -> b (cell-local
+// coordinates), as (A, Sx, Sy, Sxy) before their 1/2, 1/6, 1/6, 1/24 factors.
+__device__ __forceinline__ void seg_moments(float2 a, float2 b, float4& m) {
+    const float c = a.x * b.y - a.y * b.x;
+    m.x += c;
+    m.y += c * (a.x + b.x);
+    m.z += c * (a.y + b.y);
+    m.w += c * (2.f * a.x * a.y + a.x * b.y + b.x * a.y + 2.f * b.x * b.y);
+}
+
+// Restricts t in [t0, t1] to p + t q >= 0; false when nothing is left.
+__device__ __forceinline__ bool clip_t(float p, float q, float& t0, float& t1) {
+    if (q == 0.f) return p >= 0.f;
+    const float t = __fdividef(-p, q);
+    if (q > 0.f) t0 = fmaxf(t0, t);
+    else t1 = fminf(t1, t);
+    return t0 < t1;
+}
+
+// Sutherland-Hodgman clip of the polygon p[0..n) to one side of the unit
+// cell (axis 0: x, 1: y; hi: keep <= 1, else >= 0) into q; returns the new
+// vertex count, or -1 if it would exceed 8 (only a self-intersecting quad can).
+__device__ __forceinline__ int sh_clip(const float2* p, int n, float2* q, int axis, bool hi) {
+    int m = 0;
+    for (int i = 0; i < n; ++i) {
+        const float2 a = p[i], b = p[i + 1 == n ? 0 : i + 1];
+        const float ac = axis ? a.y : a.x, bc = axis ? b.y : b.x;
+        const bool ain = hi ? ac <= 1.f : ac >= 0.f, bin = hi ? bc <= 1.f : bc >= 0.f;
+        if (ain) {
+            if (m == 8) return -1;
+            q[m++] = a;
+        }
+        if (ain != bin) {
+            if (m == 8) return -1;
+            const float t = hi ? (ac - 1.f) / (ac - bc) : ac / (ac - bc);
+            q[m++] = axis ? make_float2(a.x + t * (b.x - a.x), hi ? 1.f : 0.f)
+                          : make_float2(hi ? 1.f : 0.f, a.y + t * (b.y - a.y));
+        }
+    }
+    return m;
+}
+
+// The reference's polygon clipping, kept for footprints whose corner rays meet
+// the splat plane on both sides (the quad then is not convex): clip against
+// x >= 0, x <= 1, y >= 0, y <= 1, then sum the polygon's edge terms.
+static __device__ __noinline__ float4 aniso_cell_polygon(const AnisoFoot F, int u, int v) {
+    float2 p[8], q[8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) p[i] = make_float2(F.s[i].x - (float)u, F.s[i].y - (float)v);
+    int n = 4;
+    const float4 none = make_float4(0.f, 0.f, 0.f, 0.f);
+    if ((n = sh_clip(p, n, q, 0, false)) < 3) return none;
+    if ((n = sh_clip(q, n, p, 0, true)) < 3) return none;
+    if ((n = sh_clip(p, n, q, 1, false)) < 3) return none;
+    if ((n = sh_clip(q, n, p, 1, true)) < 3) return none;
+    float4 m = none;
+    for (int i = 0; i < n; ++i) seg_moments(p[i], p[i + 1 == n ? 0 : i + 1], m);
+    return make_float4(m.x * 0.5f, m.y * (1.f / 6.f), m.z * (1.f / 6.f), m.w * (1.f / 24.f));
+}
+
+// Moments (A, Sx, Sy, Sxy) of the footprint quad clipped to texel cell
+// [u, u+1] x [v, v+1], in cell-local coordinates (the reference's
+// clip_and_compute_moments, filters/anisotropic_bilinear.cuh:58-190).  The
+// reference clips the quad polygon Sutherland-Hodgman style into local arrays;
+// for a convex quad (every footprint whose corner rays meet the splat plane on
+// one side) the clipped polygon's boundary is summed piecewise here instead --
+// the quad's edges clipped to the cell plus the cell's edges clipped to the
+// quad -- the same polygon's moments without dynamically indexed storage.  A
+// cell edge lying on a quad edge of the same direction is left to the quad
+// edge (counted once); of opposite direction, both count and cancel.
+__device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
+    const float2 c = make_float2((float)u + 0.5f, (float)v + 0.5f);
+    bool inside = true;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) inside = inside && (sub2(F.s[i], c).x * F.n[i].x + sub2(F.s[i], c).y * F.n[i].y >= F.nmax[i]);
+    if (inside) return make_float4(1.f, 0.5f, 0.5f, 0.25f);  // the reference's fast path: the whole cell
+    if (!F.convex) return aniso_cell_polygon(F, u, v);
+    const float fu = (float)u, fv = (float)v;
+    float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {  // quad edges inside the cell
+        const float2 a = make_float2(F.s[i].x - fu, F.s[i].y - fv), d = F.e[i];
+        float t0 = 0.f, t1 = 1.f;
+        if (clip_t(a.x, d.x, t0, t1) && clip_t(1.f - a.x, -d.x, t0, t1) && clip_t(a.y, d.y, t0, t1) &&
+            clip_t(1.f - a.y, -d.y, t0, t1))
+            seg_moments(make_float2(a.x + t0 * d.x, a.y + t0 * d.y), make_float2(a.x + t1 * d.x, a.y + t1 * d.y), m);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {  // cell edges inside the quad, counter-clockwise
+        const float2 a = make_float2((j == 1 || j == 2) ? 1.f : 0.f, j >= 2 ? 1.f : 0.f);
+        const float2 d = make_float2(j == 0 ? 1.f : (j == 2 ? -1.f : 0.f), j == 1 ? 1.f : (j == 3 ? -1.f : 0.f));
+        float t0 = 0.f, t1 = 1.f;
+        bool keep = true;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 r = make_float2(a.x + fu - F.s[i].x, a.y + fv - F.s[i].y);
+            const float p = cross2(F.e[i], r), q = cross2(F.e[i], d);
+            if (q == 0.f) keep = keep && (p > 0.f || (p == 0.f && F.e[i].x * d.x + F.e[i].y * d.y < 0.f));
+            else keep = keep && clip_t(p, q, t0, t1);
+        }
+        if (keep && t0 < t1)
+            seg_moments(make_float2(a.x + t0 * d.x, a.y + t0 * d.y), make_float2(a.x + t1 * d.x, a.y + t1 * d.y), m);
+    }
+    return make_float4(m.x * 0.5f, m.y * (1.f / 6.f), m.z * (1.f / 6.f), m.w * (1.f / 24.f));
+}
+
+// Bilinear weights of a cell's four texels (u,v), (u+1,v), (u,v+1), (u+1,v+1) from its moments.
+__device__ __forceinline__ float4 cell_weights(float4 mo) {
+    return make_float4(((mo.x - mo.y) - mo.z) + mo.w, mo.y - mo.w, mo.z - mo.w, mo.w);
+}
+
+// The texture integrated over the footprint (not yet divided by the area).
+template <class Tex>
+__device__ __forceinline__ float4 aniso_integrate(const AnisoFoot& F, const void* textures, int64_t tex_base, int rx,
+                                                  float scale) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int v = F.minv; v < F.maxv; ++v)
+        for (int u = F.minu; u < F.maxu; ++u) {
+            const float4 mo = aniso_cell(F, u, v);
+            if (mo.x == 0.f && mo.y == 0.f && mo.z == 0.f && mo.w == 0.f) continue;
+            const float4 w = cell_weights(mo);
+            const int64_t t00 = tex_base + (int64_t)v * rx + u;
+            const float4 a = Tex::load(textures, t00, scale), b = Tex::load(textures, t00 + 1, scale);
+            const float4 c = Tex::load(textures, t00 + rx, scale), d = Tex::load(textures, t00 + rx + 1, scale);
+            acc.x += a.x * w.x + b.x * w.y + c.x * w.z + d.x * w.w;
+            acc.y += a.y * w.x + b.y * w.y + c.y * w.z + d.y * w.w;
+            acc.z += a.z * w.x + b.z * w.y + c.z * w.z + d.z * w.w;
+            acc.w += a.w * w.x + b.w * w.y + c.w * w.z + d.w * w.w;
+        }
+    return acc;
+}
+
+// Adds g * weight to the gradient of every texel the footprint integrates (g already divided by the area).
+__device__ __forceinline__ void aniso_scatter(const AnisoFoot& F, float* vt, int rx, float4 g) {
+    for (int v = F.minv; v < F.maxv; ++v)
+        for (int u = F.minu; u < F.maxu; ++u) {
+            const float4 mo = aniso_cell(F, u, v);
+            if (mo.x == 0.f && mo.y == 0.f && mo.z == 0.f && mo.w == 0.f) continue;
+            const float4 w = cell_weights(mo);
+            float4* t00 = reinterpret_cast<float4*>(vt + 4 * ((int64_t)v * rx + u));
+            atomicAdd(t00, make_float4(g.x * w.x, g.y * w.x, g.z * w.x, g.w * w.x));
+            atomicAdd(t00 + 1, make_float4(g.x * w.y, g.y * w.y, g.z * w.y, g.w * w.y));
+            atomicAdd(t00 + rx, make_float4(g.x * w.z, g.y * w.z, g.z * w.z, g.w * w.z));
+            atomicAdd(t00 + rx + 1, make_float4(g.x * w.w, g.y * w.w, g.z * w.w, g.w * w.w));
+        }
+}
 
 // Coarse pyramid levels of the mip filter for one splat.  Pyramid coordinate
 // mc addresses the reference's per-splat pyramid [coarse levels | level 0]:
@@ -105,7 +318,7 @@ __device__ __forceinline__ bool mip2_taps(float sx, float sy, float dxx, float d
 // Splat data staged in shared memory: xyo = (x, y, opacity, texture scale),
 // m0/m1/m2 = rows of the ray transform (w unused).
 template <class Tex, class Filt = FiltBilinear>
-__device__ __forceinline__ void eval_pair(PairEvalT<Filt::kTaps>& e, float px, float py, const float4 xyo,
+__device__ __forceinline__ void eval_pair(PairOf<Filt>& e, float px, float py, const float4 xyo,
                                           const float4 m0, const float4 m1, const float4 m2, const void* textures,
                                           int64_t tex_base, int rx, int ry, float range_x, float range_y,
                                           float g_weight, const MipSrc mip = MipSrc{nullptr, 0, 0, 0}) {
@@ -123,7 +336,47 @@ __device__ __forceinline__ void eval_pair(PairEvalT<Filt::kTaps>& e, float px, f
     const float iz = 1.f / e.z.z;
     e.sx = e.z.x * iz;
     e.sy = e.z.y * iz;
-    if constexpr (Filt::kMip) {
+    if constexpr (Filt::kAniso) {
+        // s at the pixel's four corners (fwd.cu:296-320): the texture-space footprint quad
+        const f3 m2v = mk3(m2.x, m2.y, m2.z);
+        const f3 hx = 0.5f * cross(e.hu, m2v), hy = 0.5f * cross(e.hv, m2v);
+        const f3 c0 = (e.z - hx) - hy, c1 = (e.z + hx) - hy, c2 = (e.z + hx) + hy, c3 = (e.z - hx) + hy;
+        if (c0.z == 0.f || c1.z == 0.f || c2.z == 0.f || c3.z == 0.f) {
+            e.valid = false;
+            return;
+        }
+        e.g3 = e.sx * e.sx + e.sy * e.sy;
+        e.dx = xyo.x - px;
+        e.dy = xyo.y - py;
+        e.g2 = kFilterInvSquare * (e.dx * e.dx + e.dy * e.dy);
+        const float sigma = 0.5f * fminf(e.g3, e.g2);
+        e.kern = __expf(-sigma);
+        e.vis = 0.998f - g_weight + g_weight * e.kern;
+        e.asf = 0.f;
+        // the untextured alpha is tested before the footprint is sampled (fwd.cu:358-366)
+        const float a0 = xyo.z * e.vis;
+        if (sigma < 0.f || a0 < 1.f / 255.f) {
+            e.valid = false;
+            return;
+        }
+        const float ku = (float)(rx - 1) / (range_x * 2.f), kv = (float)(ry - 1) / (range_y * 2.f);
+        e.F.s[0] = make_float2((c0.x / c0.z + range_x) * ku, (c0.y / c0.z + range_y) * kv);
+        e.F.s[1] = make_float2((c1.x / c1.z + range_x) * ku, (c1.y / c1.z + range_y) * kv);
+        e.F.s[2] = make_float2((c2.x / c2.z + range_x) * ku, (c2.y / c2.z + range_y) * kv);
+        e.F.s[3] = make_float2((c3.x / c3.z + range_x) * ku, (c3.y / c3.z + range_y) * kv);
+        e.F.convex = (c0.z > 0.f) == (c1.z > 0.f) && (c0.z > 0.f) == (c2.z > 0.f) && (c0.z > 0.f) == (c3.z > 0.f);
+        const float area = aniso_setup(e.F, rx, ry);
+        // no texture sample: the reference zeroes alpha (fwd.cu:384-387)
+        if (!(area == 0.f || e.F.minu == e.F.maxu || e.F.minv == e.F.maxv)) {
+            e.F.iarea = 1.f / area;
+            e.tsum = aniso_integrate<Tex>(e.F, textures, tex_base, rx, xyo.w);
+            e.asf = e.tsum.w * e.F.iarea;
+            e.tex_valid = true;
+        }
+        e.alpha = fminf(0.999f, a0 * e.asf);
+        if (e.alpha < 1.f / 255.f) e.valid = false;
+        return;
+    } else if constexpr (Filt::kMip) {
         // s at the pixel's left/right and top/bottom edge midpoints: the texture-space footprint
         const f3 hw = mk3(0.5f * m2.x, 0.5f * m2.y, 0.5f * m2.z);
         const f3 cx0 = cross(e.hu - hw, e.hv), cx1 = cross(e.hu + hw, e.hv);
@@ -203,10 +456,13 @@ __device__ __forceinline__ void eval_pair(PairEvalT<Filt::kTaps>& e, float px, f
 // to pixel space through the splat's homography pixel(s) = (M0.(s,1),
 // M1.(s,1)) / M2.(s,1); when M2.(s,1) has one sign at all four corners the
 // image is a bounded convex quadrilateral, whose corners' box bounds it.
-// Otherwise (or if no bound on sigma exists) the box is unbounded.  The box is
+// Otherwise (or if no bound on sigma exists) the box is unbounded.  The
+// anisotropic_bilinear filter tests opac * vis >= 1/255 before any texture
+// term, so for it (tex_square = false) the texture square drops out.  The box is
 // widened by a margin that covers FP32 rounding of the pair evaluation.
 __device__ __forceinline__ float4 cull_box(const float4 xyo, const float4 m0, const float4 m1, const float4 m2,
-                                           bool textured, float range_x, float range_y, float g_weight) {
+                                           bool textured, float range_x, float range_y, float g_weight,
+                                           bool tex_square = true) {
     const float4 all = make_float4(-INFINITY, -INFINITY, INFINITY, INFINITY);
     const float opac = xyo.z;
     float K;  // lower bound on exp(-sigma) for a valid pair outside the texture square
@@ -221,8 +477,8 @@ __device__ __forceinline__ float4 cull_box(const float4 xyo, const float4 m0, co
     const float sig1 = K >= 1.f ? 0.f : -logf(K) * 1.001f + 1e-3f;
     const float rs = sqrtf(2.f * sig1);   // half-side of the UV square around the Gaussian disk
     const float rd = sqrtf(sig1);         // radius of the 2D-filter disk, pixels
-    const float hx = textured ? fmaxf(rs, range_x) : rs;
-    const float hy = textured ? fmaxf(rs, range_y) : rs;
+    const float hx = textured && tex_square ? fmaxf(rs, range_x) : rs;
+    const float hy = textured && tex_square ? fmaxf(rs, range_y) : rs;
     float x0 = xyo.x - rd, x1 = xyo.x + rd, y0 = xyo.y - rd, y1 = xyo.y + rd;
     int pos = 0, neg = 0;
 #pragma unroll
@@ -259,6 +515,18 @@ __device__ __forceinline__ float tex_color(const PairEvalT<NT>& e, int k) {
 #pragma unroll
     for (int i = 0; i < NT; ++i) s += e.w[i] * f4get(e.tx[i], k);
     return s;
+}
+__device__ __forceinline__ float tex_color(const PairEvalAniso& e, int k) {
+    return (k >= 4 || !e.tex_valid) ? 0.f : f4get(e.tsum, k) * e.F.iarea;
+}
+
+// The texture colour the adjoint uses: the forward's, except that the
+// anisotropic_bilinear adjoint of the reference omits the division by the
+// footprint area (bwd.cu:499-522 with filters/anisotropic_bilinear.cuh:372-389).
+template <int NT>
+__device__ __forceinline__ float tex_color_adj(const PairEvalT<NT>& e, int k) { return tex_color(e, k); }
+__device__ __forceinline__ float tex_color_adj(const PairEvalAniso& e, int k) {
+    return (k >= 4 || !e.tex_valid) ? 0.f : f4get(e.tsum, k);
 }
 
 // Sum over the lanes in `mask`; lanes outside it contribute zero.  The

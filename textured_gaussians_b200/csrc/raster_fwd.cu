@@ -137,7 +137,7 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
                 s_m1[slot] = make_float4(m[3], m[4], m[5], 0.f);
                 s_m2[slot] = make_float4(m[6], m[7], m[8], 0.f);
                 s_box[slot] = cull_box(s_xyo[slot], s_m0[slot], s_m1[slot], s_m2[slot], kTextured, a.range_x, a.range_y,
-                                       a.g_weight);
+                                       a.g_weight, !Filt::kAniso);
                 const float* n = a.normals + 3 * (int64_t)g;
                 s_nrm[slot] = make_float4(n[0], n[1], n[2], 0.f);
 #pragma unroll
@@ -162,7 +162,7 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
 #pragma unroll
             for (int q = 0; q < PPT; ++q) {
                 if (done[q] || !in_box(box, px[q], py[q])) continue;
-                PairEvalT<Filt::kTaps> e;
+                PairOf<Filt> e;
                 eval_pair<Tex, Filt>(e, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx, a.tex_ry,
                                      a.range_x, a.range_y, a.g_weight,
                                      MipSrc{a.tex_coarse, (int64_t)row * mip_clen, mip_clen, a.mip_levels});
@@ -248,18 +248,18 @@ __global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kern
 
 size_t fwd_smem_bytes(int D, int bs) { return (size_t)bs * (6 * sizeof(float4) + D * sizeof(float) + sizeof(int)); }
 
-// mipmapped2 filter: one pixel per thread (8x8 / 16x16 tiles), one CTA per tile
-template <int D, class Tex>
-cudaError_t launch_fwd_mip(const tg_raster_fwd_args& a, cudaStream_t s) {
+// mipmapped2 / anisotropic_bilinear filters: one pixel per thread (8x8 / 16x16 tiles), one CTA per tile
+template <int D, class Tex, class Filt>
+cudaError_t launch_fwd_filter(const tg_raster_fwd_args& a, cudaStream_t s) {
     const int tile_px = a.tile_size * a.tile_size;
     const int bs = a.batch_depth > 0 ? a.batch_depth : tile_px;
     const size_t smem = fwd_smem_bytes(D, bs);
     const int64_t blocks = a.views ? a.n_tiles : (int64_t)a.C * a.tile_width * a.tile_height;
     if (blocks == 0) return cudaSuccess;
-    cudaError_t err = cudaFuncSetAttribute(raster_fwd_kernel<D, Tex, 1, false, FiltMip2>,
+    cudaError_t err = cudaFuncSetAttribute(raster_fwd_kernel<D, Tex, 1, false, Filt>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
-    raster_fwd_kernel<D, Tex, 1, false, FiltMip2><<<(unsigned)blocks, tile_px, smem, s>>>(a, bs, blocks);
+    raster_fwd_kernel<D, Tex, 1, false, Filt><<<(unsigned)blocks, tile_px, smem, s>>>(a, bs, blocks);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -267,9 +267,10 @@ cudaError_t launch_fwd_mip(const tg_raster_fwd_args& a, cudaStream_t s) {
 template <int D, class Tex>
 cudaError_t launch_fwd_t(const tg_raster_fwd_args& a, cudaStream_t s) {
     if constexpr ((D == 3 || D == 4) && (Tex::kFormat == TG_TEX_F32 || Tex::kFormat == TG_TEX_BF16)) {
-        if (a.mip_levels > 0) return launch_fwd_mip<D, Tex>(a, s);
+        if (a.mip_levels > 0) return launch_fwd_filter<D, Tex, FiltMip2>(a, s);
+        if (a.filter == TG_FILTER_ANISO_BILINEAR) return launch_fwd_filter<D, Tex, FiltAniso>(a, s);
     }
-    if (a.mip_levels > 0) return cudaErrorInvalidValue;
+    if (a.mip_levels > 0 || a.filter != TG_FILTER_BILINEAR) return cudaErrorInvalidValue;
     const int tile_px = a.tile_size * a.tile_size;
     const int bs = a.batch_depth > 0 ? a.batch_depth : tile_px;
     const size_t smem = fwd_smem_bytes(D, bs);

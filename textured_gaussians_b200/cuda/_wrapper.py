@@ -37,8 +37,10 @@ _FILTER_ADJOINT = {
     "bilinear_bwd2": B.TG_ADJ_BWD2,
     "bilinear_exact": B.TG_ADJ_EXACT,
     "mipmapped2": B.TG_ADJ_REFERENCE,
+    "anisotropic_bilinear": B.TG_ADJ_REFERENCE,
 }
 _MIP_FILTERS = ("mipmapped2",)
+_FILTER_CODE = {"mipmapped2": B.TG_FILTER_MIPMAPPED2, "anisotropic_bilinear": B.TG_FILTER_ANISO_BILINEAR}
 
 
 def _bit_width(n: int) -> int:
@@ -614,7 +616,8 @@ def generate_mipmap(textures: Tensor, log_texture_res: int, log_reduce: int = 4,
 
 def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_store, tex_scales, range_x, range_y,
               backgrounds, masks, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-              gs_contrib_threshold, g_weight, C, N, layout=None, n_isects_dev=None, mip_levels=0, tex_coarse=None):
+              gs_contrib_threshold, g_weight, C, N, layout=None, n_isects_dev=None, mip_levels=0, tex_coarse=None,
+              filter_code=0):
     D = colors.shape[-1]
     vt = None if layout is None else layout.get("view_table")
     th, tw = (1, 1) if vt is not None else isect_offsets.shape[1:3]
@@ -634,7 +637,8 @@ def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_stor
         None if vt is None else B.ptr(vt.views), None if vt is None else B.ptr(vt.tile_view),
         0 if vt is None else vt.n_tiles, 0 if vt is None else vt.n_pixels, B.ptr(n_isects_dev),
         0 if layout is None else layout.get("batch_depth", 0),
-        None if layout is None else B.ptr(layout.get("work_queue")), int(mip_levels), B.ptr(tex_coarse))
+        None if layout is None else B.ptr(layout.get("work_queue")), int(mip_levels), B.ptr(tex_coarse),
+        int(filter_code))
 
 
 class _RasterizeToPixelsTextured(torch.autograd.Function):
@@ -647,13 +651,16 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
     _RasterizeToPixelsMip2TexturedGaussians) the forward builds the coarse
     levels of the FP32 textures, and the backward folds their gradient into
     the texture gradient in place (no full-pyramid tensor in either pass).
+    ``filter_code`` TG_FILTER_ANISO_BILINEAR selects the anisotropic_bilinear
+    filter (reference _RasterizeToPixelsTexturedGaussians with the
+    ``aniso_bilinear`` kernels).
     """
 
     @staticmethod
     def forward(ctx, means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, masks,
                 tex_store, tex_scales, range_x, range_y, width, height, tile_size, isect_offsets, flatten_ids,
                 absgrad, gs_contrib_threshold, g_weight, adjoint, bg_grad_index_ok, gaussian_ids, n_rows, layout,
-                mip_levels=0):
+                mip_levels=0, filter_code=0):
         dev = means2d.device
         coarse = _coarse_pyramid(textures, mip_levels) if mip_levels else None
         vt = None if layout is None else layout.get("view_table")
@@ -668,7 +675,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         n_dev = getattr(flatten_ids, "_tg_n_isects", None)
         a = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
                       backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
-                      gs_contrib_threshold, g_weight, C, N, layout, n_dev, mip_levels, coarse)
+                      gs_contrib_threshold, g_weight, C, N, layout, n_dev, mip_levels, coarse, filter_code)
         render_colors = torch.empty(pshape + (D,), dtype=torch.float32, device=dev)
         render_alphas = torch.empty(pshape + (1,), dtype=torch.float32, device=dev)
         render_normals = torch.empty(pshape + (3,), dtype=torch.float32, device=dev)
@@ -691,7 +698,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
                    gs_contrib_threshold, N, n_contrib, C, pshape)
         ctx.layout = layout
         ctx.n_isects_dev = n_dev
-        ctx.mip = (mip_levels, coarse)
+        ctx.mip = (mip_levels, coarse, filter_code)
         ctx.mark_non_differentiable(contrib_sum, contrib_count)
         return render_colors, render_alphas, render_normals, render_distort, render_median, contrib_sum, contrib_count
 
@@ -753,7 +760,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
             v_textures = v_textures.to(textures.dtype)
         return (v_means2d, v_ray_transforms, v_colors, v_opacities, v_textures, v_normals, v_densify, v_backgrounds,
                 None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None, None,
-                None, None)
+                None, None, None)
 
 
 def _layout(tile_order, view_table, batch_depth=0, persistent=False, device=None):
@@ -854,6 +861,7 @@ def rasterize_to_pixels_textured_gaussians(
         raise Exception(f"Unsupported filter type {filtering}")
     assert textures.dim() == 4 and textures.shape[-1] == 4, textures.shape
     mip_levels = mip_levels_of(textures) if filtering in _MIP_FILTERS else 0
+    filter_code = _FILTER_CODE.get(filtering, B.TG_FILTER_BILINEAR)
     if packed:
         if gaussian_ids is None:
             raise ValueError("packed textured rasterization needs gaussian_ids (texture row of each packed entry)")
@@ -876,7 +884,7 @@ def rasterize_to_pixels_textured_gaussians(
         float(texture_range_x), float(texture_range_y), int(image_width), int(image_height), int(tile_size),
         isect_offsets.contiguous(), flatten_ids.contiguous(), absgrad, gs_contrib_threshold, g_weight,
         _FILTER_ADJOINT[filtering], False, gaussian_ids, textures.shape[0],
-        _layout(tile_order, view_table, batch_depth, persistent, means2d.device), mip_levels)
+        _layout(tile_order, view_table, batch_depth, persistent, means2d.device), mip_levels, filter_code)
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]
