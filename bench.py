@@ -132,14 +132,19 @@ class ClockSampler:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.first = threading.Event()
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi's start-up (NVML initialisation) can stall the driver for tens of ms: let it finish
+            # before any timed work
+            self.first.wait(timeout=10)
         except OSError:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
+            self.first.set()
             if self.marked:  # only samples taken from the timed region on
                 self.rows.append([x.strip() for x in line.split(",")])
 

@@ -44,6 +44,7 @@ struct PairEvalT {
     float g3, g2, kern, vis, alpha, asf;
     float w[NT];
     float4 tx[NT];  // the RGBA taps
+    float4 trgba;   // the filtered texture: sum over taps of w * tap (asf = its alpha)
     int toff[NT];   // bilinear: texel index in the splat's texture; mip: pyramid coordinate (see MipSrc)
     bool valid, tex_valid;
 };
@@ -315,6 +316,20 @@ __device__ __forceinline__ bool mip2_taps(float sx, float sy, float dxx, float d
     return true;
 }
 
+// sum over taps of w[i] * tap[i], per channel, accumulated in tap order
+template <int NT>
+__device__ __forceinline__ float4 filter_taps(const float (&w)[NT], const float4 (&tx)[NT]) {
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+        s.x += w[i] * tx[i].x;
+        s.y += w[i] * tx[i].y;
+        s.z += w[i] * tx[i].z;
+        s.w += w[i] * tx[i].w;
+    }
+    return s;
+}
+
 // Splat data staged in shared memory: xyo = (x, y, opacity, texture scale),
 // m0/m1/m2 = rows of the ray transform (w unused).
 template <class Tex, class Filt = FiltBilinear>
@@ -388,15 +403,14 @@ __device__ __forceinline__ void eval_pair(PairOf<Filt>& e, float px, float py, c
         const float dxx = cx1.x / cx1.z - cx0.x / cx0.z, dxy = cx1.y / cx1.z - cx0.y / cx0.z;
         const float dyx = cy1.x / cy1.z - cy0.x / cy0.z, dyy = cy1.y / cy1.z - cy0.y / cy0.z;
         if (mip2_taps(e.sx, e.sy, dxx, dxy, dyx, dyy, rx, mip.L, range_x, range_y, e.toff, e.w)) {
-            float asf = 0.f;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const int mc = e.toff[i];
                 e.tx[i] = mc < mip.clen ? __ldg(reinterpret_cast<const float4*>(mip.coarse) + mip.cbase + mc)
                                         : Tex::load(textures, tex_base + (mc - mip.clen), xyo.w);
-                asf += e.w[i] * e.tx[i].w;
             }
-            e.asf = asf;
+            e.trgba = filter_taps<8>(e.w, e.tx);
+            e.asf = e.trgba.w;
             e.tex_valid = true;
         }
     } else if (kTextured) {
@@ -419,10 +433,8 @@ __device__ __forceinline__ void eval_pair(PairOf<Filt>& e, float px, float py, c
             e.toff[3] = vh * rx + uh;
 #pragma unroll
             for (int i = 0; i < 4; ++i) e.tx[i] = Tex::load(textures, tex_base + e.toff[i], xyo.w);
-            float asf = 0.f;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) asf += e.w[i] * e.tx[i].w;
-            e.asf = asf;
+            e.trgba = filter_taps<4>(e.w, e.tx);
+            e.asf = e.trgba.w;
             e.tex_valid = true;
         }
     }
@@ -510,11 +522,7 @@ __device__ __forceinline__ bool in_box(const float4 b, float px, float py) {
 // Texture contribution to colour channel k (channels >= 4 have none).
 template <int NT>
 __device__ __forceinline__ float tex_color(const PairEvalT<NT>& e, int k) {
-    if (k >= 4 || !e.tex_valid) return 0.f;
-    float s = 0.f;
-#pragma unroll
-    for (int i = 0; i < NT; ++i) s += e.w[i] * f4get(e.tx[i], k);
-    return s;
+    return (k >= 4 || !e.tex_valid) ? 0.f : f4get(e.trgba, k);
 }
 __device__ __forceinline__ float tex_color(const PairEvalAniso& e, int k) {
     return (k >= 4 || !e.tex_valid) ? 0.f : f4get(e.tsum, k) * e.F.iarea;

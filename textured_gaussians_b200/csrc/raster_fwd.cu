@@ -194,13 +194,14 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
                     ++ccount;
                 }
             }
-            const unsigned m = __ballot_sync(wmask, ccount > 0);
-            if (m) {
-                const float s = warp_sum(csum, wmask);
-                const float c = warp_sum((float)ccount, wmask);
+            if (__any_sync(wmask, ccount > 0)) {
+                // one-instruction warp sums: the alphas (each < 1, at most PPT per lane) in 2^-24 fixed point,
+                // so 32 lanes' sums fit in 32 bits; the quantisation is at the FP32 rounding level of the sum
+                const unsigned s = __reduce_add_sync(wmask, __float2uint_rn(csum * 16777216.f));
+                const unsigned c = __reduce_add_sync(wmask, (unsigned)ccount);
                 if (lane == __ffs(wmask) - 1) {
-                    atomicAdd(a.contrib_sum + row, s);
-                    atomicAdd(a.contrib_count + row, c);
+                    atomicAdd(a.contrib_sum + row, (float)s * (1.f / 16777216.f));
+                    atomicAdd(a.contrib_count + row, (float)c);
                 }
             }
         }
