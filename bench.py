@@ -287,6 +287,7 @@ def _run_ours(args, rank, world, local, dev):
             t0.record()
             for i in range(steps):
                 starts[i].record()
+                out = None  # the previous step's outputs are released before this step allocates its own
                 out, _ = step(storage, tile_size, per_view, depth, filtering=filtering)
                 ends[i].record()
             t1.record()
