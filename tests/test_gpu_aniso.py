@@ -6,7 +6,9 @@ restated; the kernel sums the same clipped polygon's boundary piecewise).
 Tolerances: the oracle evaluated in FP64 on the same FP32 inputs; 1e-5
 absolute per forward output with a 1e-3 fraction of branch flips (cell ranges
 are floor / ceil of footprint corners, the fast path a >= test), gradients to
-1e-4 relative L2 per tensor plus the elementwise flip budget.
+1e-4 relative L2 per tensor plus the elementwise flip budget.  Contribution
+counts per Gaussian: at most 1 % of the Gaussians (at least one) off, by at
+most 2 (pairs at the 1/255 alpha cut).
 """
 import numpy as np
 import pytest
@@ -78,7 +80,9 @@ def test_aniso_forward(name, tile, fmt):
     assert_close(rn, o.normals, 1e-5, 1e-5, frac, "normals")
     assert_close(rd, o.distort, 1e-5, 1e-4, frac, "distort")
     assert_close(rm, o.median, 1e-5, 1e-5, frac, "median")
-    assert_close(cc, o.contrib_count, 0, 0, frac, "contrib_count")
+    # a pair at the 1/255 alpha cut flips on a rounding-level change of the filtered alpha: count flips, not drift
+    nflip = int((cc != o.contrib_count).sum())
+    assert nflip <= max(1, 0.01 * cc.size) and np.abs(cc - o.contrib_count).max() <= 2, nflip
     assert rel_l2(rc, o.colors) < 1e-4
     b = rasterize_to_pixels_textured_gaussians(
         d["means2d"], d["M"], T(d["colors"]), T(d["opac"]), d["tex"], 3.0, 3.0, d["normals"],

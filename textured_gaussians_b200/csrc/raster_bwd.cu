@@ -59,10 +59,11 @@ struct GradSlots {
 #define TG_BWD_MIN_CTAS 2
 #endif
 // Register budget: TG_BWD_MIN_CTAS resident CTAs for one pixel per thread,
-// one CTA of 256 threads for the four-pixel (32x32 tile) form.
-template <int PPT>
+// one CTA of 256 threads for the four-pixel (32x32 tile) form and for the
+// anisotropic_bilinear filter (its footprint state and broadcast footprint).
+template <int PPT, class Filt>
 struct BwdBounds {
-    static constexpr int kMinCtas = PPT == 1 ? TG_BWD_MIN_CTAS : 1;
+    static constexpr int kMinCtas = Filt::kAniso ? 1 : (PPT == 1 ? TG_BWD_MIN_CTAS : 1);
 };
 
 // Per-pixel state of the back-to-front sweep.
@@ -86,7 +87,9 @@ template <int D, class Tex, class Filt = FiltBilinear>
 __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, const PairOf<Filt>& e,
                                                 PixelAdj<D>& P, const float4 xyo, const float4 nn, const float* cp,
                                                 int32_t idx, float* vt, float uv_scale, float (&vals)[32],
-                                                float* vct = nullptr, int mip_clen = 0) {
+                                                float* vct = nullptr, int mip_clen = 0, float4* aniso_g = nullptr) {
+    // aniso_g (anisotropic_bilinear): receives the texel-gradient factor of the pair (divided by the area), which
+    // the warp scatters over the footprint together
     constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
     using GS = GradSlots<D>;
     const tg_raster_fwd_args& f = a.f;
@@ -150,8 +153,7 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
                                          D > 2 ? fac * P.v_c[D > 2 ? 2 : 0] : 0.f,
                                          (D > 3 ? fac * P.v_c[D > 3 ? 3 : 0] : 0.f) + tex_a_grad);
             const float ia = e.F.iarea;
-            if (g.x != 0.f || g.y != 0.f || g.z != 0.f || g.w != 0.f)
-                aniso_scatter(e.F, vt, f.tex_rx, make_float4(g.x * ia, g.y * ia, g.z * ia, g.w * ia));
+            *aniso_g = make_float4(g.x * ia, g.y * ia, g.z * ia, g.w * ia);
         }
     } else if (kTextured && e.tex_valid && vt != nullptr) {
 #pragma unroll
@@ -361,6 +363,24 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
             bool any = false;
 #pragma unroll
             for (int q = 0; q < PPT; ++q) {
+                if constexpr (Filt::kAniso) {  // every lane takes part: the warp integrates footprints together
+                    const bool act = P[q].inside && idx <= P[q].bin_final && in_box(box, P[q].px, P[q].py);
+                    PairOf<Filt> e;
+                    eval_aniso_coop<Tex>(e, act, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx,
+                                         f.tex_ry, f.range_x, f.range_y, f.g_weight, wmask);
+                    const bool use = act && e.valid;
+                    float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (use) {
+                        any = true;
+                        accumulate_pair<D, Tex, Filt>(a, e, P[q], xyo, nn, cp, idx, vt, uv_scale, vals, vct, mip_clen,
+                                                      &g4);
+                    }
+                    aniso_coop_scatter(e.F, g4,
+                                       use && e.tex_valid && vt != nullptr &&
+                                           (g4.x != 0.f || g4.y != 0.f || g4.z != 0.f || g4.w != 0.f),
+                                       vt, f.tex_rx, wmask);
+                    continue;
+                }
                 if (!(P[q].inside && idx <= P[q].bin_final) || !in_box(box, P[q].px, P[q].py)) continue;
                 PairOf<Filt> e;
                 eval_pair<Tex, Filt>(e, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx,
@@ -397,7 +417,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
 // CTA per work item, or (work_queue != NULL) a persistent grid whose CTAs take
 // items from the queue counter until none is left.
 template <int D, class Tex, int PPT, bool kPersistent, class Filt = FiltBilinear>
-__global__ void __launch_bounds__(256, BwdBounds<PPT>::kMinCtas) raster_bwd_kernel(const tg_raster_bwd_args a,
+__global__ void __launch_bounds__(256, BwdBounds<PPT, Filt>::kMinCtas) raster_bwd_kernel(const tg_raster_bwd_args a,
                                                                                    const float uv_scale,
                                                                                    const int bs,
                                                                                    const int64_t n_items) {

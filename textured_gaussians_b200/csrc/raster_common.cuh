@@ -64,6 +64,8 @@ struct AnisoFoot {
 struct PairEvalAniso : PairEvalT<1> {
     AnisoFoot F;
     float4 tsum;
+    float a0;   // opacity x Gaussian weight: the alpha before the texture term
+    bool need;  // the footprint has texel cells to integrate
 };
 template <class Filt> struct PairOfT { using type = PairEvalT<Filt::kTaps>; };
 template <> struct PairOfT<FiltAniso> { using type = PairEvalAniso; };
@@ -216,41 +218,6 @@ __device__ __forceinline__ float4 cell_weights(float4 mo) {
     return make_float4(((mo.x - mo.y) - mo.z) + mo.w, mo.y - mo.w, mo.z - mo.w, mo.w);
 }
 
-// The texture integrated over the footprint (not yet divided by the area).
-template <class Tex>
-__device__ __forceinline__ float4 aniso_integrate(const AnisoFoot& F, const void* textures, int64_t tex_base, int rx,
-                                                  float scale) {
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int v = F.minv; v < F.maxv; ++v)
-        for (int u = F.minu; u < F.maxu; ++u) {
-            const float4 mo = aniso_cell(F, u, v);
-            if (mo.x == 0.f && mo.y == 0.f && mo.z == 0.f && mo.w == 0.f) continue;
-            const float4 w = cell_weights(mo);
-            const int64_t t00 = tex_base + (int64_t)v * rx + u;
-            const float4 a = Tex::load(textures, t00, scale), b = Tex::load(textures, t00 + 1, scale);
-            const float4 c = Tex::load(textures, t00 + rx, scale), d = Tex::load(textures, t00 + rx + 1, scale);
-            acc.x += a.x * w.x + b.x * w.y + c.x * w.z + d.x * w.w;
-            acc.y += a.y * w.x + b.y * w.y + c.y * w.z + d.y * w.w;
-            acc.z += a.z * w.x + b.z * w.y + c.z * w.z + d.z * w.w;
-            acc.w += a.w * w.x + b.w * w.y + c.w * w.z + d.w * w.w;
-        }
-    return acc;
-}
-
-// Adds g * weight to the gradient of every texel the footprint integrates (g already divided by the area).
-__device__ __forceinline__ void aniso_scatter(const AnisoFoot& F, float* vt, int rx, float4 g) {
-    for (int v = F.minv; v < F.maxv; ++v)
-        for (int u = F.minu; u < F.maxu; ++u) {
-            const float4 mo = aniso_cell(F, u, v);
-            if (mo.x == 0.f && mo.y == 0.f && mo.z == 0.f && mo.w == 0.f) continue;
-            const float4 w = cell_weights(mo);
-            float4* t00 = reinterpret_cast<float4*>(vt + 4 * ((int64_t)v * rx + u));
-            atomicAdd(t00, make_float4(g.x * w.x, g.y * w.x, g.z * w.x, g.w * w.x));
-            atomicAdd(t00 + 1, make_float4(g.x * w.y, g.y * w.y, g.z * w.y, g.w * w.y));
-            atomicAdd(t00 + rx, make_float4(g.x * w.z, g.y * w.z, g.z * w.z, g.w * w.z));
-            atomicAdd(t00 + rx + 1, make_float4(g.x * w.w, g.y * w.w, g.z * w.w, g.w * w.w));
-        }
-}
 
 // Coarse pyramid levels of the mip filter for one splat.  Pyramid coordinate
 // mc addresses the reference's per-splat pyramid [coarse levels | level 0]:
@@ -381,16 +348,11 @@ __device__ __forceinline__ void eval_pair(PairOf<Filt>& e, float px, float py, c
         e.F.s[3] = make_float2((c3.x / c3.z + range_x) * ku, (c3.y / c3.z + range_y) * kv);
         e.F.convex = (c0.z > 0.f) == (c1.z > 0.f) && (c0.z > 0.f) == (c2.z > 0.f) && (c0.z > 0.f) == (c3.z > 0.f);
         const float area = aniso_setup(e.F, rx, ry);
+        e.a0 = a0;
         // no texture sample: the reference zeroes alpha (fwd.cu:384-387)
-        if (!(area == 0.f || e.F.minu == e.F.maxu || e.F.minv == e.F.maxv)) {
-            e.F.iarea = 1.f / area;
-            e.tsum = aniso_integrate<Tex>(e.F, textures, tex_base, rx, xyo.w);
-            e.asf = e.tsum.w * e.F.iarea;
-            e.tex_valid = true;
-        }
-        e.alpha = fminf(0.999f, a0 * e.asf);
-        if (e.alpha < 1.f / 255.f) e.valid = false;
-        return;
+        e.need = !(area == 0.f || e.F.minu == e.F.maxu || e.F.minv == e.F.maxv);
+        if (e.need) e.F.iarea = 1.f / area;
+        return;  // the footprint is integrated by the warp together (eval_aniso_coop)
     } else if constexpr (Filt::kMip) {
         // s at the pixel's left/right and top/bottom edge midpoints: the texture-space footprint
         const f3 hw = mk3(0.5f * m2.x, 0.5f * m2.y, 0.5f * m2.z);
@@ -452,6 +414,142 @@ __device__ __forceinline__ void eval_pair(PairOf<Filt>& e, float px, float py, c
         e.alpha = fminf(0.999f, xyo.z * e.vis);
     }
     if (sigma < 0.f || e.alpha < 1.f / 255.f) e.valid = false;
+}
+
+// ---------------------------------------------------------------- anisotropic_bilinear, warp-cooperative
+// A pair's footprint can span anything from one texel cell to the whole
+// texture, so a lane per pixel integrating its own footprint leaves most lanes
+// idle behind the largest one (measured: 4.5 of 32 lanes active per
+// instruction).  Instead the warp integrates the footprints of its lanes one
+// after another, each footprint's cells spread over all 32 lanes (the
+// footprint is broadcast from its lane) and the partial sums reduced.
+
+__device__ __forceinline__ AnisoFoot shfl_foot(const AnisoFoot& F, int src, unsigned mask) {
+    AnisoFoot G;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        G.s[i] = make_float2(__shfl_sync(mask, F.s[i].x, src), __shfl_sync(mask, F.s[i].y, src));
+        G.e[i] = make_float2(__shfl_sync(mask, F.e[i].x, src), __shfl_sync(mask, F.e[i].y, src));
+        G.n[i] = make_float2(__shfl_sync(mask, F.n[i].x, src), __shfl_sync(mask, F.n[i].y, src));
+        G.nmax[i] = __shfl_sync(mask, F.nmax[i], src);
+    }
+    G.minu = __shfl_sync(mask, F.minu, src);
+    G.maxu = __shfl_sync(mask, F.maxu, src);
+    G.minv = __shfl_sync(mask, F.minv, src);
+    G.maxv = __shfl_sync(mask, F.maxv, src);
+    G.iarea = __shfl_sync(mask, F.iarea, src);
+    G.convex = __shfl_sync(mask, (int)F.convex, src) != 0;
+    return G;
+}
+
+__device__ __forceinline__ float4 warp_allsum4(float4 v, unsigned mask) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(mask, v.x, o);
+        v.y += __shfl_xor_sync(mask, v.y, o);
+        v.z += __shfl_xor_sync(mask, v.z, o);
+        v.w += __shfl_xor_sync(mask, v.w, o);
+    }
+    return v;
+}
+
+// Cell i of the footprint's bounding cell range, row-major.
+__device__ __forceinline__ void foot_cell(const AnisoFoot& F, int i, int& u, int& v) {
+    const int wu = F.maxu - F.minu;
+    const int r = i / wu;
+    v = F.minv + r;
+    u = F.minu + (i - r * wu);
+}
+
+// Every lane calls this with its own footprint and whether it needs one
+// integrated; returns the lane's own integral (not yet divided by the area).
+// The warp must be full (mask = all 32 lanes).
+template <class Tex>
+__device__ __forceinline__ float4 aniso_coop_sum(const AnisoFoot& Fown, bool need, const void* textures,
+                                                 int64_t tex_base, int rx, float scale, unsigned mask) {
+    const int lane = threadIdx.x & 31;
+    float4 mine = make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned pending = __ballot_sync(mask, need);
+    while (pending) {
+        const int L = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const AnisoFoot F = shfl_foot(Fown, L, mask);
+        // a footprint wholly outside the texture has an empty (possibly inverted) cell range: no cells
+        const int n = (F.maxu > F.minu && F.maxv > F.minv) ? (F.maxu - F.minu) * (F.maxv - F.minv) : 0;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int i = lane; i < n; i += 32) {
+            int u, v;
+            foot_cell(F, i, u, v);
+            const float4 mo = aniso_cell(F, u, v);
+            if (mo.x == 0.f && mo.y == 0.f && mo.z == 0.f && mo.w == 0.f) continue;
+            const float4 w = cell_weights(mo);
+            const int64_t t00 = tex_base + (int64_t)v * rx + u;
+            const float4 a = Tex::load(textures, t00, scale), b = Tex::load(textures, t00 + 1, scale);
+            const float4 c = Tex::load(textures, t00 + rx, scale), d = Tex::load(textures, t00 + rx + 1, scale);
+            acc.x += a.x * w.x + b.x * w.y + c.x * w.z + d.x * w.w;
+            acc.y += a.y * w.x + b.y * w.y + c.y * w.z + d.y * w.w;
+            acc.z += a.z * w.x + b.z * w.y + c.z * w.z + d.z * w.w;
+            acc.w += a.w * w.x + b.w * w.y + c.w * w.z + d.w * w.w;
+        }
+        acc = warp_allsum4(acc, mask);
+        if (lane == L) mine = acc;
+    }
+    return mine;
+}
+
+// Texel-gradient scatter of every lane's footprint (gown: the lane's gradient
+// already divided by the area; need: it has one), cells spread over the warp.
+__device__ __forceinline__ void aniso_coop_scatter(const AnisoFoot& Fown, float4 gown, bool need, float* vt, int rx,
+                                                   unsigned mask) {
+    const int lane = threadIdx.x & 31;
+    unsigned pending = __ballot_sync(mask, need);
+    while (pending) {
+        const int L = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const AnisoFoot F = shfl_foot(Fown, L, mask);
+        const float4 g = make_float4(__shfl_sync(mask, gown.x, L), __shfl_sync(mask, gown.y, L),
+                                     __shfl_sync(mask, gown.z, L), __shfl_sync(mask, gown.w, L));
+        // a footprint wholly outside the texture has an empty (possibly inverted) cell range: no cells
+        const int n = (F.maxu > F.minu && F.maxv > F.minv) ? (F.maxu - F.minu) * (F.maxv - F.minv) : 0;
+        for (int i = lane; i < n; i += 32) {
+            int u, v;
+            foot_cell(F, i, u, v);
+            const float4 mo = aniso_cell(F, u, v);
+            if (mo.x == 0.f && mo.y == 0.f && mo.z == 0.f && mo.w == 0.f) continue;
+            const float4 w = cell_weights(mo);
+            float4* t00 = reinterpret_cast<float4*>(vt + 4 * ((int64_t)v * rx + u));
+            atomicAdd(t00, make_float4(g.x * w.x, g.y * w.x, g.z * w.x, g.w * w.x));
+            atomicAdd(t00 + 1, make_float4(g.x * w.y, g.y * w.y, g.z * w.y, g.w * w.y));
+            atomicAdd(t00 + rx, make_float4(g.x * w.z, g.y * w.z, g.z * w.z, g.w * w.z));
+            atomicAdd(t00 + rx + 1, make_float4(g.x * w.w, g.y * w.w, g.z * w.w, g.w * w.w));
+        }
+    }
+}
+
+// The anisotropic_bilinear pair evaluation for a whole (full) warp working on
+// one splat: every lane calls it, act = the lane has a pair to evaluate; the
+// footprints that need integrating are integrated by the warp together.
+template <class Tex>
+__device__ __forceinline__ void eval_aniso_coop(PairEvalAniso& e, bool act, float px, float py, const float4 xyo,
+                                                const float4 m0, const float4 m1, const float4 m2,
+                                                const void* textures, int64_t tex_base, int rx, int ry, float range_x,
+                                                float range_y, float g_weight, unsigned mask) {
+    e.valid = false;
+    e.need = false;
+    e.tex_valid = false;
+    if (act)
+        eval_pair<Tex, FiltAniso>(e, px, py, xyo, m0, m1, m2, textures, tex_base, rx, ry, range_x, range_y, g_weight);
+    const bool need = act && e.valid && e.need;
+    const float4 ts = aniso_coop_sum<Tex>(e.F, need, textures, tex_base, rx, xyo.w, mask);
+    if (!(act && e.valid)) return;
+    e.asf = 0.f;
+    if (need) {
+        e.tsum = ts;
+        e.tex_valid = true;
+        e.asf = ts.w * e.F.iarea;
+    }
+    e.alpha = fminf(0.999f, e.a0 * e.asf);
+    if (e.alpha < 1.f / 255.f) e.valid = false;
 }
 
 // Pixel-space box outside of which a (pixel, splat) pair is provably invalid

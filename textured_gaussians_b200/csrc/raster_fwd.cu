@@ -28,10 +28,11 @@ namespace tg {
 #endif
 
 // Register budget: 4 resident CTAs of 256 threads for one pixel per thread;
-// one CTA for the four-pixel (32x32 tile) form.
-template <int PPT>
+// one CTA for the four-pixel (32x32 tile) form; two for the
+// anisotropic_bilinear filter (its footprint state and broadcast footprint).
+template <int PPT, class Filt>
 struct FwdBounds {
-    static constexpr int kMinCtas = PPT == 1 ? TG_FWD_MIN_CTAS : 1;
+    static constexpr int kMinCtas = Filt::kAniso ? 2 : (PPT == 1 ? TG_FWD_MIN_CTAS : 1);
 };
 
 // One work item (tile) of the forward; every early return is uniform over the CTA.
@@ -161,11 +162,18 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
             int ccount = 0;
 #pragma unroll
             for (int q = 0; q < PPT; ++q) {
-                if (done[q] || !in_box(box, px[q], py[q])) continue;
+                const bool act = !done[q] && in_box(box, px[q], py[q]);
                 PairOf<Filt> e;
-                eval_pair<Tex, Filt>(e, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx, a.tex_ry,
-                                     a.range_x, a.range_y, a.g_weight,
-                                     MipSrc{a.tex_coarse, (int64_t)row * mip_clen, mip_clen, a.mip_levels});
+                if constexpr (Filt::kAniso) {  // every lane takes part: the warp integrates footprints together
+                    eval_aniso_coop<Tex>(e, act, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx,
+                                         a.tex_ry, a.range_x, a.range_y, a.g_weight, wmask);
+                    if (!act) continue;
+                } else {
+                    if (!act) continue;
+                    eval_pair<Tex, Filt>(e, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx, a.tex_ry,
+                                         a.range_x, a.range_y, a.g_weight,
+                                         MipSrc{a.tex_coarse, (int64_t)row * mip_clen, mip_clen, a.mip_levels});
+                }
                 if (!e.valid) continue;
                 const float next_T = T[q] * (1.f - e.alpha);
                 if (next_T <= 1e-4f) {
@@ -227,7 +235,7 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
 // CTA per work item, or (work_queue != NULL) a persistent grid whose CTAs take
 // items from the queue counter until none is left.
 template <int D, class Tex, int PPT, bool kPersistent, class Filt = FiltBilinear>
-__global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kernel(const tg_raster_fwd_args a,
+__global__ void __launch_bounds__(256, FwdBounds<PPT, Filt>::kMinCtas) raster_fwd_kernel(const tg_raster_fwd_args a,
                                                                                    const int bs,
                                                                                    const int64_t n_items) {
     if constexpr (!kPersistent) {
