@@ -125,18 +125,20 @@ def adjoint(seed=2, N=2_000, R=16) -> Scene:
                  far_plane=100.0, name="adjoint")
 
 
-def views8(seed=1, N=300_000, R=50, n_cams=8, width=800, height=800) -> Scene:
+def views8(seed=1, N=300_000, R=50, n_cams=8, width=800, height=800, with_textures=True) -> Scene:
+    """``with_textures=False`` leaves the 12 GB of uniform[0,1] textures to the caller (textures None,
+    ``extra["texture_res"]`` = R), e.g. to draw them on the GPU."""
     rng = np.random.default_rng(seed)
     means = rng.uniform(-1, 1, size=(N, 3))
     scales, quats, opac = _gaussians(rng, N, -4.0, 0.5)
     sh = np.concatenate([rng.uniform(0, 1, size=(N, 1, 3)), rng.normal(0, 0.05, size=(N, 15, 3))], 1)
-    textures = rng.uniform(0, 1, size=(N, R, R, 4)).astype(np.float32)
+    textures = rng.uniform(0, 1, size=(N, R, R, 4)).astype(np.float32) if with_textures else None
     dirs = fibonacci_dirs(n_cams)
     V = np.stack([look_at(4.0 * d) for d in dirs])
     K = np.stack([intrinsics(1111, width / 2, height / 2)] * n_cams)
     return Scene(means.astype(np.float32), quats.astype(np.float32), scales.astype(np.float32),
                  opac.astype(np.float32), sh.astype(np.float32), textures, V.astype(np.float32),
-                 K.astype(np.float32), width, height, 3, name="views8")
+                 K.astype(np.float32), width, height, 3, name="views8", extra={"texture_res": R})
 
 
 def mixture1m(seed=3, N=1_000_000, R=32, n_cams=4, width=1600, height=1200, radius=25.0) -> Scene:
