@@ -702,8 +702,10 @@ def _run_batch(args, dev):
         B.TIMERS.enable(False)
         return t0.elapsed_time(t1) / steps, stages, B.lib().tg_kernel_launch_count() - l0
 
+    # the workload's tuning grid: tile size in {8, 16, 32} x Gaussian batch depth in {64, 128, 256}
     (tile, depth), tune_ms = autotune_compositor(("batch", N, len(sizes)),
-                                                 lambda ts, d: step_batch(ts, "heaviest_first", d), repeats=1)
+                                                 lambda ts, d: step_batch(ts, "heaviest_first", d),
+                                                 depths=(64, 128, 256), repeats=1)
     with ClockSampler(0) as clk:
         clk.mark()
         ms_b, stages_b, launches_b = timed(lambda: step_batch(tile, "heaviest_first", depth), args.steps, args.warmup)
