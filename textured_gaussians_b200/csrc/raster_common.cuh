@@ -355,9 +355,12 @@ __device__ __forceinline__ void eval_pair(PairOf<Filt>& e, float px, float py, c
         return;  // the footprint is integrated by the warp together (eval_aniso_coop)
     } else if constexpr (Filt::kMip) {
         // s at the pixel's left/right and top/bottom edge midpoints: the texture-space footprint
+        // cross(hu +- hw, hv) = z +- cross(hw, hv) and cross(hu, hv +- hw) = z +- cross(hu, hw): two cross
+        // products instead of four (the reference forms the four directly; rounding differs at the ulp level)
         const f3 hw = mk3(0.5f * m2.x, 0.5f * m2.y, 0.5f * m2.z);
-        const f3 cx0 = cross(e.hu - hw, e.hv), cx1 = cross(e.hu + hw, e.hv);
-        const f3 cy0 = cross(e.hu, e.hv - hw), cy1 = cross(e.hu, e.hv + hw);
+        const f3 ax = cross(hw, e.hv), ay = cross(e.hu, hw);
+        const f3 cx0 = e.z - ax, cx1 = e.z + ax;
+        const f3 cy0 = e.z - ay, cy1 = e.z + ay;
         if (cx0.z == 0.f || cx1.z == 0.f || cy0.z == 0.f || cy1.z == 0.f) {
             e.valid = false;
             return;
@@ -365,9 +368,16 @@ __device__ __forceinline__ void eval_pair(PairOf<Filt>& e, float px, float py, c
         const float dxx = cx1.x / cx1.z - cx0.x / cx0.z, dxy = cx1.y / cx1.z - cx0.y / cx0.z;
         const float dyx = cy1.x / cy1.z - cy0.x / cy0.z, dyy = cy1.y / cy1.z - cy0.y / cy0.z;
         if (mip2_taps(e.sx, e.sy, dxx, dxy, dyx, dyy, rx, mip.L, range_x, range_y, e.toff, e.w)) {
+            // an integer level (e.g. t clamped to 0 under magnification): the second level's taps are the first's
+            // texels again (weight 0), so they are not fetched twice
+            const bool one_level = e.toff[4] == e.toff[0];
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const int mc = e.toff[i];
+                if (i >= 4 && one_level) {
+                    e.tx[i] = e.tx[i - 4];
+                    continue;
+                }
                 e.tx[i] = mc < mip.clen ? __ldg(reinterpret_cast<const float4*>(mip.coarse) + mip.cbase + mc)
                                         : Tex::load(textures, tex_base + (mc - mip.clen), xyo.w);
             }
