@@ -393,6 +393,8 @@ def _run_ours(args, rank, world, local, dev):
                        "stage_ms": stage_ms_f32},
         "bf16_over_fp32": round(value / value_f32, 3),
         "stage_ms": stage_ms, "per_step_ms": [round(x, 3) for x in per_bf16],
+        "median_ms_per_step": round(statistics.median(per_bf16), 3),
+        "median_value": round(pix_per_step / (statistics.median(per_bf16) / 1e3) / 1e6, 2),
         "graphed": graphed, "persistent_ms_per_step": round(pers_ms, 3), "filters": filters,
         "counts": counts, "roofline": roofline, "roofline_forward": roofline_fwd, "gpu_launches": int(launches),
         "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cpu,
