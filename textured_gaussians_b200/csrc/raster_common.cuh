@@ -179,11 +179,17 @@ static __device__ __noinline__ float4 aniso_cell_polygon(const AnisoFoot F, int 
 // edge (counted once); of opposite direction, both count and cancel.
 __device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
     const float2 c = make_float2((float)u + 0.5f, (float)v + 0.5f);
-    bool inside = true;
+    bool inside = true, outside = false;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) inside = inside && (sub2(F.s[i], c).x * F.n[i].x + sub2(F.s[i], c).y * F.n[i].y >= F.nmax[i]);
+    for (int i = 0; i < 4; ++i) {
+        const float d = sub2(F.s[i], c).x * F.n[i].x + sub2(F.s[i], c).y * F.n[i].y;  // c's depth inside edge i
+        inside = inside && d >= F.nmax[i];
+        // the whole cell beyond a (non-degenerate) edge of a convex quad: nothing to integrate
+        outside = outside || (d < -F.nmax[i] && (F.e[i].x != 0.f || F.e[i].y != 0.f));
+    }
     if (inside) return make_float4(1.f, 0.5f, 0.5f, 0.25f);  // the reference's fast path: the whole cell
     if (!F.convex) return aniso_cell_polygon(F, u, v);
+    if (outside) return make_float4(0.f, 0.f, 0.f, 0.f);
     const float fu = (float)u, fv = (float)v;
     float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
