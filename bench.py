@@ -257,7 +257,7 @@ def _run_ours(args, rank, world, local, dev):
     w_rgb = torch.randn((C, H, W, 3), generator=g, device=dev)
     w_a = torch.randn((C, H, W, 1), generator=g, device=dev)
 
-    def step(storage, tile_size, per_view, depth=0, persistent=False, filtering="bilinear"):
+    def step(storage, tile_size, per_view, depth=0, persistent=False, filtering="bilinear", tex_scales=None):
         for t in (means, quats, scales, opac, colors, tex32):
             t.grad = None
         views = [slice(c, c + 1) for c in range(C)] if per_view else [slice(0, C)]
@@ -266,14 +266,15 @@ def _run_ours(args, rank, world, local, dev):
                                                    sh_degree=0, far_plane=100.0, tile_size=tile_size,
                                                    texture_storage=storage,
                                                    tile_order=args.tile_order, batch_depth=depth,
-                                                   persistent=persistent, filtering=filtering)
+                                                   persistent=persistent, filtering=filtering,
+                                                   texture_scales=tex_scales)
             loss = (out[0] * w_rgb[v]).sum() + (out[1] * w_a[v]).sum()
             loss.backward()
         return out, loss
 
-    def timed(storage, tile_size, per_view, steps, warmup, depth=0, filtering="bilinear"):
+    def timed(storage, tile_size, per_view, steps, warmup, depth=0, filtering="bilinear", tex_scales=None):
         for _ in range(warmup):
-            step(storage, tile_size, per_view, depth, filtering=filtering)
+            step(storage, tile_size, per_view, depth, filtering=filtering, tex_scales=tex_scales)
         torch.cuda.synchronize()
         barrier(world)
         torch.cuda.synchronize()
@@ -288,7 +289,7 @@ def _run_ours(args, rank, world, local, dev):
             for i in range(steps):
                 starts[i].record()
                 out = None  # the previous step's outputs are released before this step allocates its own
-                out, _ = step(storage, tile_size, per_view, depth, filtering=filtering)
+                out, _ = step(storage, tile_size, per_view, depth, filtering=filtering, tex_scales=tex_scales)
                 ends[i].record()
             t1.record()
             torch.cuda.synchronize()
@@ -340,6 +341,20 @@ def _run_ours(args, rank, world, local, dev):
                 "value": round(C * H * W * world * args.steps / (total_f / 1e3) / 1e6, 2), "unit": "Mpix/s",
                 "ms_per_step": round(total_f / args.steps, 3), "tile_size": f_tile,
                 "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stages_f.items()}}
+
+    # the other texture storage forms of the headline configuration (same tile, depth and filter)
+    storage_forms = {}
+    if not args.no_filters:
+        for fmt in ("fp16", "fp8"):
+            st_f, sc_f = make_texture_storage(tex32.detach(), fmt)
+            total_s, _, stages_s, _, out_s = timed(st_f, tile, False, args.steps, args.warmup, depth,
+                                                   tex_scales=sc_f)
+            del out_s, st_f
+            total_s = max_over_ranks(total_s, world)
+            storage_forms[fmt] = {
+                "value": round(C * H * W * world * args.steps / (total_s / 1e3) / 1e6, 2), "unit": "Mpix/s",
+                "ms_per_step": round(total_s / args.steps, 3),
+                "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stages_s.items()}}
 
     pix_per_step = C * H * W * world
     value = pix_per_step * args.steps / (total_bf16 / 1e3) / 1e6
@@ -396,6 +411,7 @@ def _run_ours(args, rank, world, local, dev):
         "median_ms_per_step": round(statistics.median(per_bf16), 3),
         "median_value": round(pix_per_step / (statistics.median(per_bf16) / 1e3) / 1e6, 2),
         "graphed": graphed, "persistent_ms_per_step": round(pers_ms, 3), "filters": filters,
+        "storage_forms": storage_forms,
         "counts": counts, "roofline": roofline, "roofline_forward": roofline_fwd, "gpu_launches": int(launches),
         "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cpu,
     }
@@ -788,7 +804,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay timing")
-    ap.add_argument("--no-filters", action="store_true", help="skip the other texture filters' timing")
+    ap.add_argument("--no-filters", action="store_true",
+                    help="skip the timing of the other texture filters and storage forms")
     ap.add_argument("--workload", default="mixture1m", choices=["mixture1m", "batch"],
                     help="mixture1m: the headline workload; batch: 64 uneven views over 3 scenes (batching form)")
     ap.add_argument("--views", type=int, default=64, help="views of the batch workload")
