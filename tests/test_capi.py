@@ -95,3 +95,56 @@ def test_product_path_fails_loudly_without_cuda():
         pytest.skip("CUDA present")
     with pytest.raises(RuntimeError, match="CUDA"):
         isect_offset_encode(torch.zeros(4, dtype=torch.int64), 1, 2, 2)
+
+
+def test_filter_arguments_are_rejected_without_a_device():
+    """The mipmapped2 / anisotropic_bilinear checks run before any device work (host pointers stand in for
+    device buffers: nothing is dereferenced before the checks fail)."""
+    L = B.lib()
+    buf = (ctypes.c_float * 4096)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+
+    def base():
+        a = B.RasterFwdArgs()
+        a.C, a.N, a.D, a.width, a.height, a.tile_size, a.tile_width, a.tile_height = 1, 4, 3, 16, 16, 16, 1, 1
+        a.n_isects = 0
+        a.means2d = a.ray_transforms = a.colors = a.opacities = a.normals = a.tile_offsets = p
+        a.tex_format, a.textures, a.tex_ry, a.tex_rx, a.range_x, a.range_y = B.TG_TEX_F32, p, 8, 8, 3.0, 3.0
+        return a
+
+    def rejected(a, code, text):
+        assert L.tg_rasterize_fwd(ctypes.byref(a), None) == code
+        assert text in L.tg_last_error(), L.tg_last_error()
+
+    a = base()
+    a.mip_levels = 14
+    rejected(a, -1, b"mip_levels")
+    a = base()
+    a.mip_levels = 2  # textures 8 x 8 are 2^3, not 2^2
+    a.tex_coarse = p
+    rejected(a, -1, b"2^L x 2^L")
+    a = base()
+    a.mip_levels = 3
+    rejected(a, -1, b"coarse pyramid")
+    a.tex_coarse, a.tile_size, a.width, a.height = p, 32, 32, 32
+    rejected(a, -2, b"tile 8 or 16")
+    a = base()
+    a.filter = 7
+    rejected(a, -1, b"unknown filter")
+    a = base()
+    a.filter = B.TG_FILTER_MIPMAPPED2
+    rejected(a, -1, b"needs mip_levels")
+    a = base()
+    a.filter, a.tex_format, a.tex_scales = B.TG_FILTER_ANISO_BILINEAR, B.TG_TEX_FP8_E4M3, p
+    rejected(a, -2, b"FP32 and BF16")
+    a = base()
+    a.filter, a.mip_levels, a.tex_coarse = B.TG_FILTER_ANISO_BILINEAR, 3, p
+    rejected(a, -1, b"no mip levels")
+    a = base()
+    a.filter, a.work_queue = B.TG_FILTER_ANISO_BILINEAR, p
+    rejected(a, -2, b"one CTA per tile")
+    # pyramid entry points: level count out of range
+    assert L.tg_generate_mipmap(p, p, 1, 0, None) == -1
+    assert L.tg_generate_mipmap(p, p, 1, 14, None) == -1
+    assert L.tg_generate_mipmap_bwd(p, p, 1, 14, None) == -1
+    assert L.tg_generate_mipmap(p, p, 0, 3, None) == 0  # no textures: nothing to do
