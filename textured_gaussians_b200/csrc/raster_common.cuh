@@ -55,7 +55,8 @@ using PairEval = PairEvalT<4>;
 // reference's edge normals and fast-path margins, the texel-cell range and
 // 1 / area; tsum is the texture integral before the division by the area.
 struct AnisoFoot {
-    float2 s[4], e[4], n[4];
+    float2 s[4], n[4];
+    float2 r[4];  // 1 / x and 1 / y of edge i, s[i+1] - s[i] (the clip divisors; unused where a component is 0)
     float nmax[4];
     int minu, maxu, minv, maxv;
     float iarea;
@@ -86,8 +87,12 @@ __device__ __forceinline__ float aniso_setup(AnisoFoot& F, int rx, int ry) {
         F.s[1] = F.s[3];
         F.s[3] = t;
     }
+    float2 e[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) F.e[i] = sub2(F.s[(i + 1) & 3], F.s[i]);
+    for (int i = 0; i < 4; ++i) {
+        e[i] = sub2(F.s[(i + 1) & 3], F.s[i]);
+        F.r[i] = make_float2(__frcp_rn(e[i].x), __frcp_rn(e[i].y));
+    }
     // float -> int conversions saturate (NaN -> 0), so the cell range stays within the texture
     F.minu = max(0, (int)floorf(fminf(fminf(F.s[0].x, F.s[1].x), fminf(F.s[2].x, F.s[3].x))));
     F.maxu = min(rx - 1, (int)ceilf(fmaxf(fmaxf(F.s[0].x, F.s[1].x), fmaxf(F.s[2].x, F.s[3].x))));
@@ -97,8 +102,8 @@ __device__ __forceinline__ float aniso_setup(AnisoFoot& F, int rx, int ry) {
     const float cy = (((F.s[0].y + F.s[1].y) + F.s[2].y) + F.s[3].y) * 0.25f;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        float2 n = (F.e[i].x == 0.f && F.e[i].y == 0.f) ? make_float2(F.s[i].x - cx, F.s[i].y - cy)
-                                                        : make_float2(F.e[i].y, -F.e[i].x);
+        float2 n = (e[i].x == 0.f && e[i].y == 0.f) ? make_float2(F.s[i].x - cx, F.s[i].y - cy)
+                                                    : make_float2(e[i].y, -e[i].x);
         const float l = sqrtf(n.x * n.x + n.y * n.y);
         if (l != 0.f) n = make_float2(n.x / l, n.y / l);
         F.n[i] = n;
@@ -117,10 +122,10 @@ __device__ __forceinline__ void seg_moments(float2 a, float2 b, float4& m) {
     m.w += c * (2.f * a.x * a.y + a.x * b.y + b.x * a.y + 2.f * b.x * b.y);
 }
 
-// Restricts t in [t0, t1] to p + t q >= 0; false when nothing is left.
-__device__ __forceinline__ bool clip_t(float p, float q, float& t0, float& t1) {
+// Restricts t in [t0, t1] to p + t q >= 0 (rq = 1 / q); false when nothing is left.
+__device__ __forceinline__ bool clip_t(float p, float q, float rq, float& t0, float& t1) {
     if (q == 0.f) return p >= 0.f;
-    const float t = __fdividef(-p, q);
+    const float t = -p * rq;
     if (q > 0.f) t0 = fmaxf(t0, t);
     else t1 = fminf(t1, t);
     return t0 < t1;
@@ -179,13 +184,16 @@ static __device__ __noinline__ float4 aniso_cell_polygon(const AnisoFoot F, int 
 // edge (counted once); of opposite direction, both count and cancel.
 __device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
     const float2 c = make_float2((float)u + 0.5f, (float)v + 0.5f);
+    float2 e[4];  // the quad's edges, formed again here rather than held across the cell loop
+#pragma unroll
+    for (int i = 0; i < 4; ++i) e[i] = sub2(F.s[(i + 1) & 3], F.s[i]);
     bool inside = true, outside = false;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const float d = sub2(F.s[i], c).x * F.n[i].x + sub2(F.s[i], c).y * F.n[i].y;  // c's depth inside edge i
         inside = inside && d >= F.nmax[i];
         // the whole cell beyond a (non-degenerate) edge of a convex quad: nothing to integrate
-        outside = outside || (d < -F.nmax[i] && (F.e[i].x != 0.f || F.e[i].y != 0.f));
+        outside = outside || (d < -F.nmax[i] && (e[i].x != 0.f || e[i].y != 0.f));
     }
     if (inside) return make_float4(1.f, 0.5f, 0.5f, 0.25f);  // the reference's fast path: the whole cell
     if (!F.convex) return aniso_cell_polygon(F, u, v);
@@ -194,10 +202,10 @@ __device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
     float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {  // quad edges inside the cell
-        const float2 a = make_float2(F.s[i].x - fu, F.s[i].y - fv), d = F.e[i];
+        const float2 a = make_float2(F.s[i].x - fu, F.s[i].y - fv), d = e[i], rd = F.r[i];
         float t0 = 0.f, t1 = 1.f;
-        if (clip_t(a.x, d.x, t0, t1) && clip_t(1.f - a.x, -d.x, t0, t1) && clip_t(a.y, d.y, t0, t1) &&
-            clip_t(1.f - a.y, -d.y, t0, t1))
+        if (clip_t(a.x, d.x, rd.x, t0, t1) && clip_t(1.f - a.x, -d.x, -rd.x, t0, t1) &&
+            clip_t(a.y, d.y, rd.y, t0, t1) && clip_t(1.f - a.y, -d.y, -rd.y, t0, t1))
             seg_moments(make_float2(a.x + t0 * d.x, a.y + t0 * d.y), make_float2(a.x + t1 * d.x, a.y + t1 * d.y), m);
     }
 #pragma unroll
@@ -209,9 +217,11 @@ __device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const float2 r = make_float2(a.x + fu - F.s[i].x, a.y + fv - F.s[i].y);
-            const float p = cross2(F.e[i], r), q = cross2(F.e[i], d);
-            if (q == 0.f) keep = keep && (p > 0.f || (p == 0.f && F.e[i].x * d.x + F.e[i].y * d.y < 0.f));
-            else keep = keep && clip_t(p, q, t0, t1);
+            const float p = cross2(e[i], r), q = cross2(e[i], d);
+            // q is -e.y, e.x, e.y, -e.x for the cell edges j = 0..3: its reciprocal is the footprint's
+            const float rq = j == 0 ? -F.r[i].y : (j == 1 ? F.r[i].x : (j == 2 ? F.r[i].y : -F.r[i].x));
+            if (q == 0.f) keep = keep && (p > 0.f || (p == 0.f && e[i].x * d.x + e[i].y * d.y < 0.f));
+            else keep = keep && clip_t(p, q, rq, t0, t1);
         }
         if (keep && t0 < t1)
             seg_moments(make_float2(a.x + t0 * d.x, a.y + t0 * d.y), make_float2(a.x + t1 * d.x, a.y + t1 * d.y), m);
@@ -445,7 +455,7 @@ __device__ __forceinline__ AnisoFoot shfl_foot(const AnisoFoot& F, int src, unsi
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         G.s[i] = make_float2(__shfl_sync(mask, F.s[i].x, src), __shfl_sync(mask, F.s[i].y, src));
-        G.e[i] = make_float2(__shfl_sync(mask, F.e[i].x, src), __shfl_sync(mask, F.e[i].y, src));
+        G.r[i] = make_float2(__shfl_sync(mask, F.r[i].x, src), __shfl_sync(mask, F.r[i].y, src));
         G.n[i] = make_float2(__shfl_sync(mask, F.n[i].x, src), __shfl_sync(mask, F.n[i].y, src));
         G.nmax[i] = __shfl_sync(mask, F.nmax[i], src);
     }
