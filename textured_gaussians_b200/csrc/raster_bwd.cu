@@ -60,11 +60,16 @@ struct GradSlots {
 #endif
 // Register budget: TG_BWD_MIN_CTAS resident CTAs for one pixel per thread,
 // one CTA of 256 threads for the four-pixel (32x32 tile) form.  The
-// anisotropic_bilinear adjoint keeps this budget too: at 128 registers it
-// spills ~0.5 KB but runs 28 % faster than unconstrained at 245 (measured).
-template <int PPT>
+// anisotropic_bilinear adjoint keeps this budget too (TG_BWD_MIN_CTAS_ANISO):
+// at 128 registers it spills ~0.5 KB but runs 28 % faster than unconstrained
+// at 245; at 85 it gains 1.5 % for twice the spills, at 64 it loses 17 %
+// (1M splats, 4 views, measured).
+#ifndef TG_BWD_MIN_CTAS_ANISO
+#define TG_BWD_MIN_CTAS_ANISO TG_BWD_MIN_CTAS
+#endif
+template <int PPT, class Filt>
 struct BwdBounds {
-    static constexpr int kMinCtas = PPT == 1 ? TG_BWD_MIN_CTAS : 1;
+    static constexpr int kMinCtas = PPT == 1 ? (Filt::kAniso ? TG_BWD_MIN_CTAS_ANISO : TG_BWD_MIN_CTAS) : 1;
 };
 
 // Per-pixel state of the back-to-front sweep.
@@ -367,7 +372,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
                 if constexpr (Filt::kAniso) {  // every lane takes part: the warp integrates footprints together
                     const bool act = P[q].inside && idx <= P[q].bin_final && in_box(box, P[q].px, P[q].py);
                     PairOf<Filt> e;
-                    eval_aniso_coop<Tex>(e, act, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx,
+                    eval_aniso_coop<Tex, true>(e, act, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx,
                                          f.tex_ry, f.range_x, f.range_y, f.g_weight, wmask);
                     const bool use = act && e.valid;
                     float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -376,7 +381,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
                         accumulate_pair<D, Tex, Filt>(a, e, P[q], xyo, nn, cp, idx, vt, uv_scale, vals, vct, mip_clen,
                                                       &g4);
                     }
-                    aniso_coop_scatter(e.F, g4,
+                    aniso_coop_scatter<true>(e.F, g4,
                                        use && e.tex_valid && vt != nullptr &&
                                            (g4.x != 0.f || g4.y != 0.f || g4.z != 0.f || g4.w != 0.f),
                                        vt, f.tex_rx, wmask);
@@ -418,7 +423,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
 // CTA per work item, or (work_queue != NULL) a persistent grid whose CTAs take
 // items from the queue counter until none is left.
 template <int D, class Tex, int PPT, bool kPersistent, class Filt = FiltBilinear>
-__global__ void __launch_bounds__(256, BwdBounds<PPT>::kMinCtas) raster_bwd_kernel(const tg_raster_bwd_args a,
+__global__ void __launch_bounds__(256, BwdBounds<PPT, Filt>::kMinCtas) raster_bwd_kernel(const tg_raster_bwd_args a,
                                                                                    const float uv_scale,
                                                                                    const int bs,
                                                                                    const int64_t n_items) {

@@ -172,37 +172,17 @@ static __device__ __noinline__ float4 aniso_cell_polygon(const AnisoFoot F, int 
     return make_float4(m.x * 0.5f, m.y * (1.f / 6.f), m.z * (1.f / 6.f), m.w * (1.f / 24.f));
 }
 
-// Moments (A, Sx, Sy, Sxy) of the footprint quad clipped to texel cell
-// [u, u+1] x [v, v+1], in cell-local coordinates (the reference's
-// clip_and_compute_moments, filters/anisotropic_bilinear.cuh:58-190).  The
-// reference clips the quad polygon Sutherland-Hodgman style into local arrays;
-// for a convex quad (every footprint whose corner rays meet the splat plane on
-// one side) the clipped polygon's boundary is summed piecewise here instead --
-// the quad's edges clipped to the cell plus the cell's edges clipped to the
-// quad -- the same polygon's moments without dynamically indexed storage.  A
-// cell edge lying on a quad edge of the same direction is left to the quad
-// edge (counted once); of opposite direction, both count and cancel.
-__device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
-    const float2 c = make_float2((float)u + 0.5f, (float)v + 0.5f);
-    float2 e[4];  // the quad's edges, formed again here rather than held across the cell loop
+// The piecewise boundary sum of a convex quad (corners s, counter-clockwise;
+// rc: reciprocals of its edges' components) over cell [u, u+1] x [v, v+1].
+__device__ __forceinline__ float4 cell_edges_sum(const float2 (&s)[4], const float2 (&rc)[4], int u, int v) {
+    float2 e[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) e[i] = sub2(F.s[(i + 1) & 3], F.s[i]);
-    bool inside = true, outside = false;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const float d = sub2(F.s[i], c).x * F.n[i].x + sub2(F.s[i], c).y * F.n[i].y;  // c's depth inside edge i
-        inside = inside && d >= F.nmax[i];
-        // the whole cell beyond a (non-degenerate) edge of a convex quad: nothing to integrate
-        outside = outside || (d < -F.nmax[i] && (e[i].x != 0.f || e[i].y != 0.f));
-    }
-    if (inside) return make_float4(1.f, 0.5f, 0.5f, 0.25f);  // the reference's fast path: the whole cell
-    if (!F.convex) return aniso_cell_polygon(F, u, v);
-    if (outside) return make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = 0; i < 4; ++i) e[i] = sub2(s[(i + 1) & 3], s[i]);
     const float fu = (float)u, fv = (float)v;
     float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {  // quad edges inside the cell
-        const float2 a = make_float2(F.s[i].x - fu, F.s[i].y - fv), d = e[i], rd = F.r[i];
+        const float2 a = make_float2(s[i].x - fu, s[i].y - fv), d = e[i], rd = rc[i];
         float t0 = 0.f, t1 = 1.f;
         if (clip_t(a.x, d.x, rd.x, t0, t1) && clip_t(1.f - a.x, -d.x, -rd.x, t0, t1) &&
             clip_t(a.y, d.y, rd.y, t0, t1) && clip_t(1.f - a.y, -d.y, -rd.y, t0, t1))
@@ -216,10 +196,10 @@ __device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
         bool keep = true;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const float2 r = make_float2(a.x + fu - F.s[i].x, a.y + fv - F.s[i].y);
+            const float2 r = make_float2(a.x + fu - s[i].x, a.y + fv - s[i].y);
             const float p = cross2(e[i], r), q = cross2(e[i], d);
             // q is -e.y, e.x, e.y, -e.x for the cell edges j = 0..3: its reciprocal is the footprint's
-            const float rq = j == 0 ? -F.r[i].y : (j == 1 ? F.r[i].x : (j == 2 ? F.r[i].y : -F.r[i].x));
+            const float rq = j == 0 ? -rc[i].y : (j == 1 ? rc[i].x : (j == 2 ? rc[i].y : -rc[i].x));
             if (q == 0.f) keep = keep && (p > 0.f || (p == 0.f && e[i].x * d.x + e[i].y * d.y < 0.f));
             else keep = keep && clip_t(p, q, rq, t0, t1);
         }
@@ -227,6 +207,47 @@ __device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
             seg_moments(make_float2(a.x + t0 * d.x, a.y + t0 * d.y), make_float2(a.x + t1 * d.x, a.y + t1 * d.y), m);
     }
     return make_float4(m.x * 0.5f, m.y * (1.f / 6.f), m.z * (1.f / 6.f), m.w * (1.f / 24.f));
+}
+
+// The same sum as one out-of-line copy.  The adjoint integrates every
+// footprint twice (its integral, then its texel gradients); with the sum
+// inlined at both places its hot code outgrew the instruction cache.
+static __device__ __noinline__ float4 cell_edges_sum_shared(float2 s0, float2 s1, float2 s2, float2 s3, float2 r0,
+                                                            float2 r1, float2 r2, float2 r3, int u, int v) {
+    const float2 s[4] = {s0, s1, s2, s3}, rc[4] = {r0, r1, r2, r3};
+    return cell_edges_sum(s, rc, u, v);
+}
+
+// Moments (A, Sx, Sy, Sxy) of the footprint quad clipped to texel cell
+// [u, u+1] x [v, v+1], in cell-local coordinates (the reference's
+// clip_and_compute_moments, filters/anisotropic_bilinear.cuh:58-190).  The
+// reference clips the quad polygon Sutherland-Hodgman style into local arrays;
+// for a convex quad (every footprint whose corner rays meet the splat plane on
+// one side) the clipped polygon's boundary is summed piecewise here instead --
+// the quad's edges clipped to the cell plus the cell's edges clipped to the
+// quad -- the same polygon's moments without dynamically indexed storage.  A
+// cell edge lying on a quad edge of the same direction is left to the quad
+// edge (counted once); of opposite direction, both count and cancel.
+// kShared: take the boundary sum from its out-of-line copy.
+template <bool kShared = false>
+__device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
+    const float2 c = make_float2((float)u + 0.5f, (float)v + 0.5f);
+    bool inside = true, outside = false;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float d = sub2(F.s[i], c).x * F.n[i].x + sub2(F.s[i], c).y * F.n[i].y;  // c's depth inside edge i
+        const float2 e = sub2(F.s[(i + 1) & 3], F.s[i]);
+        inside = inside && d >= F.nmax[i];
+        // the whole cell beyond a (non-degenerate) edge of a convex quad: nothing to integrate
+        outside = outside || (d < -F.nmax[i] && (e.x != 0.f || e.y != 0.f));
+    }
+    if (inside) return make_float4(1.f, 0.5f, 0.5f, 0.25f);  // the reference's fast path: the whole cell
+    if (!F.convex) return aniso_cell_polygon(F, u, v);
+    if (outside) return make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (kShared)
+        return cell_edges_sum_shared(F.s[0], F.s[1], F.s[2], F.s[3], F.r[0], F.r[1], F.r[2], F.r[3], u, v);
+    else
+        return cell_edges_sum(F.s, F.r, u, v);
 }
 
 // Bilinear weights of a cell's four texels (u,v), (u+1,v), (u,v+1), (u+1,v+1) from its moments.
@@ -490,7 +511,7 @@ __device__ __forceinline__ void foot_cell(const AnisoFoot& F, int i, int& u, int
 // Every lane calls this with its own footprint and whether it needs one
 // integrated; returns the lane's own integral (not yet divided by the area).
 // The warp must be full (mask = all 32 lanes).
-template <class Tex>
+template <class Tex, bool kShared = false>
 __device__ __forceinline__ float4 aniso_coop_sum(const AnisoFoot& Fown, bool need, const void* textures,
                                                  int64_t tex_base, int rx, float scale, unsigned mask) {
     const int lane = threadIdx.x & 31;
@@ -506,7 +527,7 @@ __device__ __forceinline__ float4 aniso_coop_sum(const AnisoFoot& Fown, bool nee
         for (int i = lane; i < n; i += 32) {
             int u, v;
             foot_cell(F, i, u, v);
-            const float4 mo = aniso_cell(F, u, v);
+            const float4 mo = aniso_cell<kShared>(F, u, v);
             if (mo.x == 0.f && mo.y == 0.f && mo.z == 0.f && mo.w == 0.f) continue;
             const float4 w = cell_weights(mo);
             const int64_t t00 = tex_base + (int64_t)v * rx + u;
@@ -525,6 +546,7 @@ __device__ __forceinline__ float4 aniso_coop_sum(const AnisoFoot& Fown, bool nee
 
 // Texel-gradient scatter of every lane's footprint (gown: the lane's gradient
 // already divided by the area; need: it has one), cells spread over the warp.
+template <bool kShared = false>
 __device__ __forceinline__ void aniso_coop_scatter(const AnisoFoot& Fown, float4 gown, bool need, float* vt, int rx,
                                                    unsigned mask) {
     const int lane = threadIdx.x & 31;
@@ -540,7 +562,7 @@ __device__ __forceinline__ void aniso_coop_scatter(const AnisoFoot& Fown, float4
         for (int i = lane; i < n; i += 32) {
             int u, v;
             foot_cell(F, i, u, v);
-            const float4 mo = aniso_cell(F, u, v);
+            const float4 mo = aniso_cell<kShared>(F, u, v);
             if (mo.x == 0.f && mo.y == 0.f && mo.z == 0.f && mo.w == 0.f) continue;
             const float4 w = cell_weights(mo);
             float4* t00 = reinterpret_cast<float4*>(vt + 4 * ((int64_t)v * rx + u));
@@ -555,7 +577,7 @@ __device__ __forceinline__ void aniso_coop_scatter(const AnisoFoot& Fown, float4
 // The anisotropic_bilinear pair evaluation for a whole (full) warp working on
 // one splat: every lane calls it, act = the lane has a pair to evaluate; the
 // footprints that need integrating are integrated by the warp together.
-template <class Tex>
+template <class Tex, bool kShared = false>
 __device__ __forceinline__ void eval_aniso_coop(PairEvalAniso& e, bool act, float px, float py, const float4 xyo,
                                                 const float4 m0, const float4 m1, const float4 m2,
                                                 const void* textures, int64_t tex_base, int rx, int ry, float range_x,
@@ -566,7 +588,7 @@ __device__ __forceinline__ void eval_aniso_coop(PairEvalAniso& e, bool act, floa
     if (act)
         eval_pair<Tex, FiltAniso>(e, px, py, xyo, m0, m1, m2, textures, tex_base, rx, ry, range_x, range_y, g_weight);
     const bool need = act && e.valid && e.need;
-    const float4 ts = aniso_coop_sum<Tex>(e.F, need, textures, tex_base, rx, xyo.w, mask);
+    const float4 ts = aniso_coop_sum<Tex, kShared>(e.F, need, textures, tex_base, rx, xyo.w, mask);
     if (!(act && e.valid)) return;
     e.asf = 0.f;
     if (need) {

@@ -29,11 +29,15 @@ namespace tg {
 
 // Register budget: 4 resident CTAs of 256 threads for one pixel per thread;
 // one CTA for the four-pixel (32x32 tile) form.  The anisotropic_bilinear
-// forward keeps this budget too: it spills ~0.5 KB at 64 registers but runs
-// 13 % faster than at 128 (measured).
-template <int PPT>
+// forward keeps this budget too (TG_FWD_MIN_CTAS_ANISO): it spills ~0.5 KB at
+// 64 registers but runs 13 % faster than at 128 and 3.5 % faster than at 85
+// (measured).
+#ifndef TG_FWD_MIN_CTAS_ANISO
+#define TG_FWD_MIN_CTAS_ANISO TG_FWD_MIN_CTAS
+#endif
+template <int PPT, class Filt>
 struct FwdBounds {
-    static constexpr int kMinCtas = PPT == 1 ? TG_FWD_MIN_CTAS : 1;
+    static constexpr int kMinCtas = PPT == 1 ? (Filt::kAniso ? TG_FWD_MIN_CTAS_ANISO : TG_FWD_MIN_CTAS) : 1;
 };
 
 // One work item (tile) of the forward; every early return is uniform over the CTA.
@@ -236,7 +240,7 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
 // CTA per work item, or (work_queue != NULL) a persistent grid whose CTAs take
 // items from the queue counter until none is left.
 template <int D, class Tex, int PPT, bool kPersistent, class Filt = FiltBilinear>
-__global__ void __launch_bounds__(256, FwdBounds<PPT>::kMinCtas) raster_fwd_kernel(const tg_raster_fwd_args a,
+__global__ void __launch_bounds__(256, FwdBounds<PPT, Filt>::kMinCtas) raster_fwd_kernel(const tg_raster_fwd_args a,
                                                                                    const int bs,
                                                                                    const int64_t n_items) {
     if constexpr (!kPersistent) {
