@@ -131,7 +131,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.first = threading.Event()
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -329,17 +329,19 @@ def _run_ours(args, rank, world, local, dev):
     total_f32 = max_over_ranks(total_f32, world)
     # the same headline form with the other texture filters: mipmapped2 (coarse levels built and folded back
     # every step) and anisotropic_bilinear (each pixel's footprint integrated over the texel cells it covers)
+    # (at most 5 timed steps each: an anisotropic_bilinear step takes about a second)
     filters = {}
     if not args.no_filters:
         f_tile = min(tile, 16)
+        f_steps = min(args.steps, 5)
         for filt in ("mipmapped2", "anisotropic_bilinear"):
-            total_f, _, stages_f, _, out_f = timed(store, f_tile, False, args.steps, args.warmup,
+            total_f, _, stages_f, _, out_f = timed(store, f_tile, False, f_steps, args.warmup,
                                                    depth if f_tile == tile else 0, filt)
             del out_f
             total_f = max_over_ranks(total_f, world)
             filters[filt] = {
-                "value": round(C * H * W * world * args.steps / (total_f / 1e3) / 1e6, 2), "unit": "Mpix/s",
-                "ms_per_step": round(total_f / args.steps, 3), "tile_size": f_tile,
+                "value": round(C * H * W * world * f_steps / (total_f / 1e3) / 1e6, 2), "unit": "Mpix/s",
+                "ms_per_step": round(total_f / f_steps, 3), "steps": f_steps, "tile_size": f_tile,
                 "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stages_f.items()}}
 
     # the other texture storage forms of the headline configuration (same tile, depth and filter)
@@ -791,7 +793,8 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20,
+                    help="timed steps: value from their total time, median_value from their median")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--splats", type=int, default=1_000_000)
