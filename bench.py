@@ -272,6 +272,8 @@ def _run_ours(args, rank, world, local, dev):
             loss.backward()
         return out, loss
 
+    timed_info = {}
+
     def timed(storage, tile_size, per_view, steps, warmup, depth=0, filtering="bilinear", tex_scales=None):
         for _ in range(warmup):
             step(storage, tile_size, per_view, depth, filtering=filtering, tex_scales=tex_scales)
@@ -283,6 +285,7 @@ def _run_ours(args, rank, world, local, dev):
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         l0 = B.lib().tg_kernel_launch_count()
+        seg0 = torch.cuda.memory_stats().get("segment.all.allocated", 0)
         B.TIMERS.enable(True)
         with no_gc():
             t0.record()
@@ -293,6 +296,8 @@ def _run_ours(args, rank, world, local, dev):
                 ends[i].record()
             t1.record()
             torch.cuda.synchronize()
+        # device segments the caching allocator had to add inside the timed steps (0 = every step reused memory)
+        timed_info["segments_allocated"] = torch.cuda.memory_stats().get("segment.all.allocated", 0) - seg0
         launches = B.lib().tg_kernel_launch_count() - l0
         stages = B.TIMERS.summary()
         B.TIMERS.enable(False)
@@ -316,6 +321,7 @@ def _run_ours(args, rank, world, local, dev):
             depth = int(max_over_ranks(float(depth), world))
         clk.mark()
         total_bf16, per_bf16, stages_bf16, launches, out = timed(store, tile, False, args.steps, args.warmup, depth)
+        segments_bf16 = timed_info["segments_allocated"]
     total_bf16 = max_over_ranks(total_bf16, world)
     fwd_b, bwd_b, counts = compositor_bytes(out[-1], 3, R, 2, N, C, H, W)
     del out  # no live autograd graph may reach the leaves when a CUDA graph is captured
@@ -335,13 +341,15 @@ def _run_ours(args, rank, world, local, dev):
         f_tile = min(tile, 16)
         f_steps = min(args.steps, 5)
         for filt in ("mipmapped2", "anisotropic_bilinear"):
-            total_f, _, stages_f, _, out_f = timed(store, f_tile, False, f_steps, args.warmup,
-                                                   depth if f_tile == tile else 0, filt)
+            total_f, per_f, stages_f, _, out_f = timed(store, f_tile, False, f_steps, args.warmup,
+                                                       depth if f_tile == tile else 0, filt)
             del out_f
             total_f = max_over_ranks(total_f, world)
             filters[filt] = {
                 "value": round(C * H * W * world * f_steps / (total_f / 1e3) / 1e6, 2), "unit": "Mpix/s",
                 "ms_per_step": round(total_f / f_steps, 3), "steps": f_steps, "tile_size": f_tile,
+                "per_step_ms": [round(x, 3) for x in per_f],
+                "allocator_segments_in_timed_steps": timed_info["segments_allocated"],
                 "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stages_f.items()}}
 
     # the other texture storage forms of the headline configuration (same tile, depth and filter)
@@ -410,6 +418,7 @@ def _run_ours(args, rank, world, local, dev):
                        "stage_ms": stage_ms_f32},
         "bf16_over_fp32": round(value / value_f32, 3),
         "stage_ms": stage_ms, "per_step_ms": [round(x, 3) for x in per_bf16],
+        "allocator_segments_in_timed_steps": segments_bf16,
         "median_ms_per_step": round(statistics.median(per_bf16), 3),
         "median_value": round(pix_per_step / (statistics.median(per_bf16) / 1e3) / 1e6, 2),
         "graphed": graphed, "persistent_ms_per_step": round(pers_ms, 3), "filters": filters,

@@ -60,12 +60,12 @@ struct GradSlots {
 #endif
 // Register budget: TG_BWD_MIN_CTAS resident CTAs for one pixel per thread,
 // one CTA of 256 threads for the four-pixel (32x32 tile) form.  The
-// anisotropic_bilinear adjoint keeps this budget too (TG_BWD_MIN_CTAS_ANISO):
-// at 128 registers it spills ~0.5 KB but runs 28 % faster than unconstrained
-// at 245; at 85 it gains 1.5 % for twice the spills, at 64 it loses 17 %
-// (1M splats, 4 views, measured).
+// anisotropic_bilinear adjoint targets 3 CTAs (85 registers): with its clips
+// branch-free and its cell boundary sum out of line it spills ~1 KB there but
+// runs 3.9 % faster than at 128, which was already 28 % faster than the
+// unconstrained 245; 64 registers lose 17 % (1M splats, 4 views, measured).
 #ifndef TG_BWD_MIN_CTAS_ANISO
-#define TG_BWD_MIN_CTAS_ANISO TG_BWD_MIN_CTAS
+#define TG_BWD_MIN_CTAS_ANISO 3
 #endif
 template <int PPT, class Filt>
 struct BwdBounds {
