@@ -60,7 +60,7 @@ struct GradSlots {
 #endif
 // Register budget: TG_BWD_MIN_CTAS resident CTAs for one pixel per thread,
 // one CTA of 256 threads for the four-pixel (32x32 tile) form.  The
-// anisotropic_bilinear adjoint targets 3 CTAs (85 registers): with its clips
+// anisotropic_bilinear adjoint targets 3 CTAs (80 registers allocated): with its clips
 // branch-free and its cell boundary sum out of line it spills ~1 KB there but
 // runs 3.9 % faster than at 128, which was already 28 % faster than the
 // unconstrained 245; 64 registers lose 17 % (1M splats, 4 views, measured).

@@ -30,8 +30,8 @@ namespace tg {
 // Register budget: 4 resident CTAs of 256 threads for one pixel per thread;
 // one CTA for the four-pixel (32x32 tile) form.  The anisotropic_bilinear
 // forward keeps this budget too (TG_FWD_MIN_CTAS_ANISO): it spills ~0.5 KB at
-// 64 registers but runs 13 % faster than at 128 and 3.5 % faster than at 85
-// (measured).
+// 64 registers but runs 13 % faster than at 128 and 2-3.5 % faster than at 3
+// CTAs (measured).
 #ifndef TG_FWD_MIN_CTAS_ANISO
 #define TG_FWD_MIN_CTAS_ANISO TG_FWD_MIN_CTAS
 #endif
