@@ -60,7 +60,8 @@ struct AnisoFoot {
     float nmax[4];
     int minu, maxu, minv, maxv;
     float iarea;
-    bool convex;  // the four corner rays meet the splat plane on one side (same sign of z)
+    bool convex;  // the four corner rays meet the splat plane on one side (same sign of z) and no two
+                  // adjacent corners coincide: the boundary sum applies, else the polygon clipping
 };
 struct PairEvalAniso : PairEvalT<1> {
     AnisoFoot F;
@@ -77,7 +78,8 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(
 
 // Orientation (counter-clockwise), texel-cell range, edge normals and margins
 // of the footprint quad; returns its area (precompute,
-// filters/anisotropic_bilinear.cuh:193-245).
+// filters/anisotropic_bilinear.cuh:193-245).  Clears F.convex for a quad with
+// a zero-length edge.
 __device__ __forceinline__ float aniso_setup(AnisoFoot& F, int rx, int ry) {
     float area = 0.5f * (cross2(sub2(F.s[1], F.s[0]), sub2(F.s[2], F.s[1])) +
                          cross2(sub2(F.s[3], F.s[2]), sub2(F.s[0], F.s[3])));
@@ -92,6 +94,8 @@ __device__ __forceinline__ float aniso_setup(AnisoFoot& F, int rx, int ry) {
     for (int i = 0; i < 4; ++i) {
         e[i] = sub2(F.s[(i + 1) & 3], F.s[i]);
         F.r[i] = make_float2(__frcp_rn(e[i].x), __frcp_rn(e[i].y));
+        // a zero-length edge (collapsed corner) has no half-plane: the polygon clipping handles that quad
+        if (e[i].x == 0.f && e[i].y == 0.f) F.convex = false;
     }
     // float -> int conversions saturate (NaN -> 0), so the cell range stays within the texture
     F.minu = max(0, (int)floorf(fminf(fminf(F.s[0].x, F.s[1].x), fminf(F.s[2].x, F.s[3].x))));
@@ -204,7 +208,8 @@ __device__ __forceinline__ float4 cell_edges_sum(const float2 (&s)[4], const flo
             const float p = cross2(e[i], r), q = cross2(e[i], d);
             // q is -e.y, e.x, e.y, -e.x for the cell edges j = 0..3: its reciprocal is the footprint's
             const float rq = j == 0 ? -rc[i].y : (j == 1 ? rc[i].x : (j == 2 ? rc[i].y : -rc[i].x));
-            // parallel to quad edge i (q = 0): kept if inside it, or on it running the other way
+            // parallel to quad edge i (q = 0): kept if inside it, or on it running the other way (a quad
+            // with a zero-length edge, for which this would drop every cell edge, takes the polygon clipping)
             const bool par = p > 0.f || (p == 0.f && e[i].x * d.x + e[i].y * d.y < 0.f);
             const bool k = clip_t(p, q, rq, t0, t1);
             keep = keep & (q == 0.f ? par : k);
