@@ -1,0 +1,50 @@
+"""Writes api_signatures.json: the parameter lists (name, kind, default) of the
+reference's public functions on the rasterization path, read by importing the
+reference package on the CPU (textured_gaussians/rendering.py and
+textured_gaussians/cuda/_wrapper.py; importing them needs no GPU).
+
+Run from the repository root with the reference checkout as the argument:
+
+    python tests/golden/make_api_signatures.py <path to the textured_gaussians checkout>
+"""
+import inspect
+import json
+import os
+import sys
+
+FUNCTIONS = {
+    "textured_gaussians.rendering": ["rasterization_textured_gaussians", "rasterization_2dgs"],
+    "textured_gaussians.cuda._wrapper": [
+        "spherical_harmonics", "fully_fused_projection_2dgs", "isect_tiles", "isect_offset_encode",
+        "rasterize_to_pixels_textured_gaussians", "rasterize_to_pixels_2dgs", "generate_mipmap",
+        "selective_adam_update",
+    ],
+}
+
+
+def describe(fn):
+    out = []
+    for p in inspect.signature(fn).parameters.values():
+        out.append({"name": p.name, "kind": p.kind.name,
+                    "default": None if p.default is inspect.Parameter.empty else repr(p.default)})
+    return out
+
+
+def main(ref_root):
+    sys.path.insert(0, ref_root)
+    import importlib
+    table = {}
+    for mod, names in FUNCTIONS.items():
+        m = importlib.import_module(mod)
+        for n in names:
+            if hasattr(m, n):
+                table[f"{mod}.{n}"] = describe(getattr(m, n))
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "api_signatures.json"), "w") as f:
+        json.dump(table, f, indent=1, sort_keys=True)
+        f.write("\n")
+    print(f"{len(table)} signatures written")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1])
