@@ -1,7 +1,8 @@
 """Writes api_signatures.json: the parameter lists (name, kind, default) of the
 reference's public functions on the rasterization path, read by importing the
 reference package on the CPU (textured_gaussians/rendering.py and
-textured_gaussians/cuda/_wrapper.py; importing them needs no GPU).
+textured_gaussians/cuda/_wrapper.py; importing them needs no GPU), and the keys
+of the ``meta`` dict each renderer returns (read from its source).
 
 Run from the repository root with the reference checkout as the argument:
 
@@ -30,6 +31,19 @@ def describe(fn):
     return out
 
 
+def meta_keys(fn):
+    """Keys of the last ``meta = {...}`` dict literal in the function's source (the renderers' ``meta``)."""
+    import ast
+    import textwrap
+    tree = ast.parse(textwrap.dedent(inspect.getsource(fn)))
+    keys = None
+    for node in ast.walk(tree):
+        if (isinstance(node, ast.Assign) and isinstance(node.value, ast.Dict)
+                and any(isinstance(t, ast.Name) and t.id == "meta" for t in node.targets)):
+            keys = [k.value for k in node.value.keys]
+    return keys
+
+
 def main(ref_root):
     sys.path.insert(0, ref_root)
     import importlib
@@ -39,11 +53,14 @@ def main(ref_root):
         for n in names:
             if hasattr(m, n):
                 table[f"{mod}.{n}"] = describe(getattr(m, n))
+    rendering = importlib.import_module("textured_gaussians.rendering")
+    for n in FUNCTIONS["textured_gaussians.rendering"]:
+        table[f"meta_keys:{n}"] = meta_keys(getattr(rendering, n))
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "api_signatures.json"), "w") as f:
         json.dump(table, f, indent=1, sort_keys=True)
         f.write("\n")
-    print(f"{len(table)} signatures written")
+    print(f"{len(table)} entries written")
 
 
 if __name__ == "__main__":
