@@ -1,6 +1,7 @@
-"""CPU checks of bench.py's roofline arithmetic: the compulsory-bytes model of
-the compositor launches and the measured-traffic lookup (which applies to the
-workload it was measured on only)."""
+"""CPU checks of bench.py: the roofline arithmetic (the compulsory-bytes model
+of the compositor launches and the measured-traffic lookup, which applies to
+the workload it was measured on only) and the reference arm's JSON line."""
+import os
 import types
 
 import torch
@@ -31,3 +32,23 @@ def test_measured_traffic_applies_to_its_workload_only():
     assert bench.traffic_bytes(args, 500_000, 4, 32, 8, 64) is None
     args.traffic_bytes = 1.5e9
     assert bench.traffic_bytes(args, 3, 1, 8, 16, 0) == 1.5e9
+
+
+def test_reference_arm_prints_the_contract_line():
+    """``bench.py --impl reference`` times the CPU oracle (no GPU needed); a reduced workload keeps this quick."""
+    import json
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "2",
+                          "--warmup", "0", "--splats", "20000", "--cameras", "1"], capture_output=True, text=True,
+                         cwd=root, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == "Mpix/s"
+    assert line["higher_is_better"] is True and line["steps"] == 2 and line["value"] > 0
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": "Mpix/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
