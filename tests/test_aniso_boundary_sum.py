@@ -70,12 +70,15 @@ def _seg(a, b, m):
     m[3] += c * (2 * a[0] * a[1] + a[0] * b[1] + b[0] * a[1] + 2 * b[0] * b[1])
 
 
-def _cell(s, e, n, nmax, u, v):
-    """Moments (A, Sx, Sy, Sxy) of the convex quad clipped to cell (u, v), cell-local (aniso_cell)."""
+def _cell(s, e, n, nmax, u, v, convex=True):
+    """Moments (A, Sx, Sy, Sxy) of the quad clipped to cell (u, v), cell-local (aniso_cell): the whole-cell fast
+    path, then the polygon clipping for a quad that is not convex, else the outside skip and the boundary sum."""
     c = np.array([u + 0.5, v + 0.5])
     d = [(s[i] - c) @ n[i] for i in range(4)]
     if all(d[i] >= nmax[i] for i in range(4)):
         return np.array([1.0, 0.5, 0.5, 0.25])
+    if not convex:
+        return _cell_polygon(s, u, v)
     if any(d[i] < -nmax[i] and (e[i] != 0).any() for i in range(4)):
         return np.zeros(4)
     m = np.zeros(4)
@@ -143,7 +146,7 @@ def boundary_sum_filter(corners, tex):
     acc = np.zeros(4)
     for v in range(minv, maxv):
         for u in range(minu, maxu):
-            mo = _cell(s, e, n, nmax, u, v) if convex else _cell_polygon(s, u, v)
+            mo = _cell(s, e, n, nmax, u, v, convex)
             w = np.array([mo[0] - mo[1] - mo[2] + mo[3], mo[1] - mo[3], mo[2] - mo[3], mo[3]])
             acc += w[0] * tex[v, u] + w[1] * tex[v, u + 1] + w[2] * tex[v + 1, u] + w[3] * tex[v + 1, u + 1]
     return acc / area if area > 0 else acc, area
