@@ -136,13 +136,15 @@ def _cell_polygon(s, u, v):
     return m * np.array([0.5, 1 / 6, 1 / 6, 1 / 24])
 
 
-def boundary_sum_filter(corners, tex):
+def boundary_sum_filter(corners, tex, convex=None):
     """The kernels' anisotropic_bilinear value of one quad over tex [ry, rx, 4]: the boundary sum for a quad
     without a zero-length edge, the polygon clipping otherwise (the quads here have corners on one side of
     the splat plane)."""
     ry, rx = tex.shape[:2]
     s, e, n, nmax, (minu, maxu, minv, maxv), area = _setup(corners, rx, ry)
-    convex = all((ei != 0).any() for ei in e)
+    if convex is None:  # the kernels also clear it when the corner rays straddle the splat plane
+        convex = all((ei != 0).any() for ei in e)
+    convex = convex and all((ei != 0).any() for ei in e)
     acc = np.zeros(4)
     for v in range(minv, maxv):
         for u in range(minu, maxu):
@@ -217,3 +219,16 @@ def test_collapsed_corner_needs_the_polygon_clipping():
             acc += w[0] * tex[v, u] + w[1] * tex[v, u + 1] + w[2] * tex[v + 1, u] + w[3] * tex[v + 1, u + 1]
     assert np.abs(acc / area - ref).max() > 1e-3
     np.testing.assert_allclose(boundary_sum_filter(q, tex)[0], ref, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("quad", [[(1.0, 1.0), (6.0, 4.0), (6.0, 1.5), (1.5, 4.5)],
+                                  [(2.2, 1.3), (6.7, 6.1), (1.4, 6.6), (6.9, 2.0)]])
+def test_self_intersecting_quads_take_the_polygon_clipping(quad):
+    """Corner rays on both sides of the splat plane give a self-intersecting quad; the kernels then use the
+    reference's polygon clipping (after the whole-cell fast path), which the oracle restates too."""
+    tex = np.random.default_rng(9).uniform(-1, 1, size=(9, 9, 4))
+    q = np.array(quad, float)
+    ref, ref_area = O.aniso_sample(q, tex)
+    out, area = boundary_sum_filter(q, tex, convex=False)
+    assert abs(area - ref_area) <= 1e-12 * max(1.0, ref_area)
+    np.testing.assert_allclose(out, ref, rtol=0, atol=1e-12)
