@@ -13,6 +13,11 @@ Parity status: projection, intersection, offsets and SH are pinned against
 golden vectors from the reference's pure-torch twins; the plain compositor is
 pinned against the reference's torch ``accumulate_2dgs``; the textured
 compositor is a restatement with no executable reference ("parity unpinned").
+Its adjoints are checked by FP64 finite differences instead: the exact
+bilinear adjoint (tests/test_adjoint_fd.py), the reference and bwd2 adjoints
+against it (tests/test_oracle_adjoint_modes.py), the mipmapped2 and
+anisotropic_bilinear adjoints (tests/test_oracle_filter_adjoint.py) and the SH
+adjoint (tests/test_oracle_sh_adjoint.py).
 """
 from __future__ import annotations
 
