@@ -274,16 +274,6 @@ TG_API size_t tg_sort_workspace_bytes(int64_t n, int32_t end_bit);
 TG_API int tg_sort_pairs(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, int64_t n, int32_t end_bit,
                   void* workspace, size_t workspace_bytes, int32_t* result_in_alt, tg_stream_t stream);
 
-/* The same sort, for callers that cannot allocate device memory (a plugin host
- * that owns all GPU memory, a real-time loop that must not call cudaMalloc, a
- * host without a caching allocator).  No counterpart in the reference.  The
- * caller passes only keys, values and their ping-pong buffers; the scratch the
- * sort needs lives in a static device array of this library (8 MiB + 16 KiB
- * held on every GPU that loads it, until exit), so n is limited to
- * TG_SORT_NOALLOC_MAX_PAIRS -- larger n is rejected with TG_ERR_INVALID_ARG.
- * Calls share that array: those that overlap on one GPU race and must be
- * serialised by the caller.  The first call on a device looks up the array's
- * address with that device current; make it before any stream capture. */
 /* Waits for `stream`, then reports whether any bounded look-back wait of the
  * last tg_sort_pairs call that used `workspace` (with the same n and end_bit)
  * gave up: TG_ERR_TIMEOUT if so, TG_OK otherwise.  Synchronising; for
@@ -300,9 +290,34 @@ TG_API int tg_sort_status(const void* workspace, int64_t n, int32_t end_bit, tg_
 TG_API int tg_sort_lookback_selftest(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt,
                                      void* workspace, size_t workspace_bytes, tg_stream_t stream);
 
+/* The same sort, for callers that cannot allocate device memory (a plugin host
+ * that owns all GPU memory, a real-time loop that must not call cudaMalloc, a
+ * host without a caching allocator).  No counterpart in the reference.  The
+ * caller passes only keys, values and their ping-pong buffers; the scratch the
+ * sort needs lives in a static device array of this library (8 MiB + 16 KiB
+ * held on every GPU that loads it, until exit), so n is limited to
+ * TG_SORT_NOALLOC_MAX_PAIRS -- larger n is rejected with TG_ERR_INVALID_ARG.
+ * Calls share that array: those that overlap on one GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the array's
+ * address with that device current; make it before any stream capture (the
+ * address is looked up again if the device's context has changed since). */
 #define TG_SORT_NOALLOC_MAX_PAIRS 4194304
 TG_API int tg_sort_pairs_noalloc(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt, int64_t n,
                                  int32_t end_bit, int32_t* result_in_alt, tg_stream_t stream);
+
+/* Waits for `stream`, then reports whether a bounded look-back wait of the last
+ * tg_sort_pairs_noalloc call on the current device gave up: TG_ERR_TIMEOUT if
+ * so, TG_OK otherwise (the flag lives in the static scratch and is cleared by
+ * every call).  Synchronising; for diagnostics and tests.  No counterpart in
+ * the reference. */
+TG_API int tg_sort_noalloc_status(tg_stream_t stream);
+
+/* tg_sort_lookback_selftest run on the static scratch of tg_sort_pairs_noalloc
+ * (8192 pairs of keys/vals into keys_alt/vals_alt): returns TG_ERR_TIMEOUT by
+ * design, and leaves the flag set for tg_sort_noalloc_status until the next
+ * sort.  No counterpart in the reference. */
+TG_API int tg_sort_noalloc_lookback_selftest(int64_t* keys, int32_t* vals, int64_t* keys_alt, int32_t* vals_alt,
+                                             tg_stream_t stream);
 
 /* Replaces isect_offset_encode_tensor (textured_gaussians/cuda/csrc/isect_tiles.cu:357-390):
  * offsets[c,ty,tx] = index of the first sorted intersection of tile (c,ty,tx)

