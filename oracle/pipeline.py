@@ -96,7 +96,7 @@ def render_backward(cache: Cache, means, quats, scales, opacities, colors, textu
     if v_normals_world is None:
         v_ncam = z((C, H, W, 3))
     else:
-        v_ncam = np.einsum("cji,chwj->chwi", cache.rot, np.asarray(v_normals_world, dt))
+        v_ncam = np.einsum("cji,chwj->chwi", cache.rot_c2w, np.asarray(v_normals_world, dt))
     g = O.raster_bwd(cache.means2d, cache.M, cache.colors, cache.opac_rep, cache.normals, textures, cache.offsets,
                      cache.flatten_ids, W, H, tile_size, cache.fwd, v_colors, v_alphas, v_ncam, v_distort, v_median,
                      range_x, range_y, backgrounds, g_weight=g_weight, mode=raster_mode, dtype=dt)
