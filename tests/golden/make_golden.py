@@ -1,7 +1,8 @@
 """Generate tests/golden/*.npz from the reference's own pure-torch code.
 
-Run in a container where the reference is mounted (read-only) at
-/root/reference:  python tests/golden/make_golden.py
+Run where the reference's source tree is mounted (read-only), naming its
+root:  python tests/golden/make_golden.py --reference PATH  (or set
+REFERENCE_ROOT).
 
 The reference's CUDA extension cannot be built (its GLM submodule is empty),
 but these pure-torch twins import and run on the CPU:
@@ -19,8 +20,8 @@ per-ray sum of weights * values).  The contributing (Gaussian, pixel) pairs fed
 to accumulate_2dgs are enumerated here in numpy, front to back, with the
 reference compositor's alpha cut (1/255) and stop rule (T <= 1e-4).
 
-The fixtures are small and committed; nothing on the GPU machine reads
-/root/reference.
+The fixtures are small and committed; nothing on the GPU machine reads the
+reference tree.
 """
 import os
 import sys
@@ -29,7 +30,16 @@ import types
 import numpy as np
 import torch
 
-REF = "/root/reference"
+def _reference_root() -> str:
+    if "--reference" in sys.argv:
+        return sys.argv[sys.argv.index("--reference") + 1]
+    root = os.environ.get("REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("name the reference's source tree: --reference PATH or REFERENCE_ROOT")
+    return root
+
+
+REF = _reference_root()
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.dont_write_bytecode = True
 sys.path.insert(0, REF)
