@@ -407,6 +407,17 @@ typedef struct {
      * (F32 / BF16 storage, 3 or 4 channels, tile 8 or 16, one CTA per tile,
      * reference adjoint). */
     int32_t filter;
+    /* Transmittance checkpoints (NULL: none; no counterpart in the reference,
+     * whose adjoint recovers each splat's transmittance by dividing the final
+     * one by (1 - alpha) back to front, rasterize_to_pixels_textured_gaussians_
+     * 2dgs_bwd.cu:160, :456-457).  When set, the forward writes every pixel's
+     * transmittance at the end of each batch of its tile, and the adjoint,
+     * given the same pointer, restarts the division from that exact value at
+     * every batch, so rounding accumulates over one batch of splats instead of
+     * the whole list.  FP32, [n_tiles + n_isects / bs + 1, tile_size^2] with
+     * bs the batch depth (tile_size^2 when batch_depth is 0); row
+     * t + tile_offsets[t] / bs + k holds batch k of tile t. */
+    float* t_checkpoints;
 } tg_raster_fwd_args;
 TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
 

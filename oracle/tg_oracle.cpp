@@ -796,9 +796,16 @@ template <typename T> inline void atomic_add(T* p, T v) {
 }
 
 // mode: 0 = reference "bilinear" adjoint, 1 = reference "bilinear_bwd2"
-//       adjoint, 2 = exact derivative of the forward.
+//       adjoint, 2 = exact derivative of the forward; plus kRecomputeT (16):
+//       the transmittance in front of each splat is the front-to-back product
+//       recomputed per pixel, instead of the reference's back-to-front division
+//       of the final transmittance by (1 - alpha)
+//       (rasterize_to_pixels_textured_gaussians_2dgs_bwd.cu:160, :456-457).
+constexpr int kRecomputeT = 16;
 template <typename T>
 void raster_bwd(const RasterIn<T>& a, const RasterGradIn<T>& gi, const RasterGradOut<T>& go, int mode, int64_t E) {
+    const bool recompute = (mode & kRecomputeT) != 0;
+    mode &= ~kRecomputeT;
     const int T_ = a.tile_w * a.tile_h;
     const int D = a.D;
     std::vector<uint8_t> touched(E, 0);
@@ -809,7 +816,7 @@ void raster_bwd(const RasterIn<T>& a, const RasterGradIn<T>& gi, const RasterGra
         const int ty = tile / a.tile_w, tx = tile % a.tile_w;
         int64_t rs, re;
         tile_range(a, c, tile, rs, re);
-        std::vector<T> buf(D), vrgb(D), texc(D);
+        std::vector<T> buf(D), vrgb(D), texc(D), t_before;
         for (int dy = 0; dy < a.tile_size; ++dy)
             for (int dx = 0; dx < a.tile_size; ++dx) {
                 const int i = ty * a.tile_size + dy, j = tx * a.tile_size + dx;
@@ -830,6 +837,17 @@ void raster_bwd(const RasterIn<T>& a, const RasterGradIn<T>& gi, const RasterGra
                 T acc_w_buf = gi.alphas[pid], acc_w = acc_w_buf;
                 T dist_buf = 0;
                 const T vmed = gi.v_median[pid];
+                if (recompute) {  // T in front of every splat of the pixel's list, front to back
+                    const int64_t last = std::min<int64_t>(bin_final, re - 1);
+                    t_before.assign(std::max<int64_t>(last - rs + 1, 0), T(1));
+                    T tf = T(1);
+                    for (int64_t idx = rs; idx <= last; ++idx) {
+                        t_before[idx - rs] = tf;
+                        SplatEval<T> e;
+                        eval_splat(a, a.flatten_ids[idx], px, py, e);
+                        if (e.valid) tf *= T(1) - e.alpha;
+                    }
+                }
                 for (int64_t idx = std::min<int64_t>(bin_final, re - 1); idx >= rs; --idx) {
                     const int64_t g = a.flatten_ids[idx];
                     SplatEval<T> e;
@@ -840,7 +858,7 @@ void raster_bwd(const RasterIn<T>& a, const RasterGradIn<T>& gi, const RasterGra
                     std::fill(vrgb.begin(), vrgb.end(), T(0));
                     if (idx == med_idx) vrgb[D - 1] += vmed;
                     const T ra = T(1) / (T(1) - e.alpha);
-                    Tr *= ra;
+                    Tr = recompute ? t_before[idx - rs] : Tr * ra;
                     const T fac = e.alpha * Tr;
                     const bool tex_on = a.textures && e.valid_tex > 0;
                     T* vtex = tex_on ? go.v_textures + tex_row(a, g) * tex_texels(a) * 4 : nullptr;

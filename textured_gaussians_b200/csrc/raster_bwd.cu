@@ -83,6 +83,16 @@ struct PixelAdj {
     float v_n[3], buf_n[3];
     int32_t bin_final, median_idx;
     float acc_d_buf, acc_d, acc_w_buf, acc_w, dist_buf;
+    int32_t local;     // pixel index within the tile
+    int32_t ck_batch;  // forward batch whose end transmittance T was last restarted from (-1: none)
+};
+
+// The forward's transmittance checkpoints of one tile (tg_raster_fwd_args.t_checkpoints): base is the tile's
+// first row, rows of `stride` pixels, forward batches of bs splats from range_start rs.  base NULL: none.
+struct TileCkpt {
+    const float* base;
+    int64_t stride;
+    int32_t rs, bs;
 };
 
 // Adds one (pixel, splat) pair's gradient contributions to the lane's per-splat
@@ -93,7 +103,8 @@ template <int D, class Tex, class Filt = FiltBilinear>
 __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, const PairOf<Filt>& e,
                                                 PixelAdj<D>& P, const float4 xyo, const float4 nn, const float* cp,
                                                 int32_t idx, float* vt, float uv_scale, float (&vals)[32],
-                                                float* vct = nullptr, int mip_clen = 0, float4* aniso_g = nullptr) {
+                                                const TileCkpt& ck, float* vct = nullptr, int mip_clen = 0,
+                                                float4* aniso_g = nullptr) {
     // aniso_g (anisotropic_bilinear): receives the texel-gradient factor of the pair (divided by the area), which
     // the warp scatters over the footprint together
     constexpr bool kTextured = Tex::kFormat != TG_TEX_NONE;
@@ -101,6 +112,16 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
     const tg_raster_fwd_args& f = a.f;
     const float opac = xyo.z;
     if (idx == P.median_idx) vals[GS::kRgb + D - 1] += P.v_med;
+    if (ck.base != nullptr) {
+        // first pair of a new forward batch (back to front): T restarts from the forward's exact value at the
+        // batch's end -- no splat after this one in the batch contributed to this pixel, or it would have
+        // been met first
+        const int32_t fb = (idx - ck.rs) / ck.bs;
+        if (fb != P.ck_batch) {
+            P.ck_batch = fb;
+            P.T = ck.base[(int64_t)fb * ck.stride + P.local];
+        }
+    }
     const float ra = 1.f / (1.f - e.alpha);
     P.T *= ra;
     const float T = P.T;
@@ -280,6 +301,8 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
         const int j = tc.tx * ts + local % ts;
         p.pix = pixel_index(tc, i, j);
         p.inside = p.pix >= 0;
+        p.local = local;
+        p.ck_batch = -1;
         p.px = (float)j + 0.5f;
         p.py = (float)i + 0.5f;
         p.T_final = 1.f; p.v_a = p.v_dist = p.v_med = p.bg_dot = 0.f;
@@ -323,6 +346,10 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
     const int32_t block_max_bin = s_max_bin;
     const int64_t tex_stride = (int64_t)f.tex_ry * f.tex_rx;
     const int mip_clen = Filt::kMip ? ((1 << (2 * f.mip_levels)) - 1) / 3 : 0;
+    const int tile_px = nt * PPT;
+    const TileCkpt ck{f.t_checkpoints != nullptr
+                          ? f.t_checkpoints + ((int64_t)tc.t + range_start / bs) * (int64_t)tile_px : nullptr,
+                      (int64_t)tile_px, range_start, bs};
 
     for (int32_t batch_end = range_end - 1; batch_end >= range_start; batch_end -= bs) {
         if (batch_end - (bs - 1) > block_max_bin) continue;  // every splat here is past all last contributors
@@ -378,8 +405,8 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
                     float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (use) {
                         any = true;
-                        accumulate_pair<D, Tex, Filt>(a, e, P[q], xyo, nn, cp, idx, vt, uv_scale, vals, vct, mip_clen,
-                                                      &g4);
+                        accumulate_pair<D, Tex, Filt>(a, e, P[q], xyo, nn, cp, idx, vt, uv_scale, vals, ck, vct,
+                                                      mip_clen, &g4);
                     }
                     aniso_coop_scatter<true>(e.F, g4,
                                        use && e.tex_valid && vt != nullptr &&
@@ -394,7 +421,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
                                      MipSrc{f.tex_coarse, (int64_t)row * mip_clen, mip_clen, f.mip_levels});
                 if (!e.valid) continue;
                 any = true;
-                accumulate_pair<D, Tex, Filt>(a, e, P[q], xyo, nn, cp, idx, vt, uv_scale, vals, vct, mip_clen);
+                accumulate_pair<D, Tex, Filt>(a, e, P[q], xyo, nn, cp, idx, vt, uv_scale, vals, ck, vct, mip_clen);
             }
             if (!__any_sync(wmask, any)) continue;
             warp_reduce_scatter32(vals, wmask);

@@ -218,6 +218,11 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
                 }
             }
         }
+        if (a.t_checkpoints != nullptr) {  // every pixel's transmittance at the end of this batch
+            float* ck = a.t_checkpoints + ((int64_t)tc.t + range_start / bs + b) * (int64_t)(nt * PPT);
+#pragma unroll
+            for (int q = 0; q < PPT; ++q) ck[tr + q * nt] = T[q];
+        }
     }
 #pragma unroll
     for (int q = 0; q < PPT; ++q) {

@@ -689,6 +689,8 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         a.out_distort, a.out_median = B.ptr(render_distort), B.ptr(render_median)
         a.last_ids, a.median_ids = B.ptr(last_ids), B.ptr(median_ids)
         a.contrib_sum, a.contrib_count = B.ptr(contrib_sum), B.ptr(contrib_count)
+        ckpt = _checkpoint_buffer(layout, isect_offsets, flatten_ids, tile_size, C, dev)
+        a.t_checkpoints = B.ptr(ckpt)
         st = B.stream_of(means2d)
         B.call("tg_rasterize_fwd", st, B.lib().tg_rasterize_fwd, ctypes.byref(a), st)
         ctx.save_for_backward(means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, m,
@@ -699,6 +701,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         ctx.layout = layout
         ctx.n_isects_dev = n_dev
         ctx.mip = (mip_levels, coarse, filter_code)
+        ctx.t_checkpoints = ckpt
         ctx.mark_non_differentiable(contrib_sum, contrib_count)
         return render_colors, render_alphas, render_normals, render_distort, render_median, contrib_sum, contrib_count
 
@@ -724,6 +727,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         f = _fwd_args(means2d, ray_transforms, colors, opacities, normals, tex_store, tex_scales, range_x, range_y,
                       backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
                       0.0, g_weight, C, N, ctx.layout, ctx.n_isects_dev, *ctx.mip)
+        f.t_checkpoints = B.ptr(ctx.t_checkpoints)
         v_means2d = torch.empty_like(means2d)
         v_means2d_abs = torch.empty_like(means2d) if absgrad else None
         v_ray_transforms = torch.empty_like(ray_transforms)
@@ -763,14 +767,32 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
                 None, None, None)
 
 
-def _layout(tile_order, view_table, batch_depth=0, persistent=False, device=None):
-    if tile_order is None and view_table is None and not batch_depth and not persistent:
+_TRANSMITTANCE = ("divide", "checkpoint")
+
+
+def _layout(tile_order, view_table, batch_depth=0, persistent=False, device=None, transmittance="divide"):
+    if transmittance not in _TRANSMITTANCE:
+        raise ValueError(f"transmittance must be one of {_TRANSMITTANCE}, got {transmittance!r}")
+    ckpt = transmittance == "checkpoint"
+    if tile_order is None and view_table is None and not batch_depth and not persistent and not ckpt:
         return None
     if tile_order is not None:
         tile_order = tile_order.to(torch.int32).contiguous()
     queue = torch.zeros((1,), dtype=torch.int32, device=device) if persistent else None
     return {"tile_order": tile_order, "view_table": view_table, "batch_depth": int(batch_depth or 0),
-            "work_queue": queue}
+            "work_queue": queue, "checkpoints": ckpt}
+
+
+def _checkpoint_buffer(layout, isect_offsets, flatten_ids, tile_size, C, device):
+    """The transmittance checkpoints of tg_raster_fwd_args: [n_tiles + n_isects / bs + 1, tile_size^2] FP32,
+    or None when the layout does not ask for them."""
+    if layout is None or not layout.get("checkpoints"):
+        return None
+    vt = layout.get("view_table")
+    n_tiles = vt.n_tiles if vt is not None else C * isect_offsets.shape[1] * isect_offsets.shape[2]
+    bs = layout.get("batch_depth") or tile_size * tile_size
+    return torch.empty((n_tiles + flatten_ids.numel() // bs + 1, tile_size * tile_size), dtype=torch.float32,
+                       device=device)
 
 
 def _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
@@ -831,6 +853,7 @@ def rasterize_to_pixels_textured_gaussians(
     view_table=None,
     batch_depth: int = 0,
     persistent: bool = False,
+    transmittance: str = "divide",
 ) -> Tuple[Tensor, ...]:
     """Rasterize textured 2D Gaussians to pixels (reference: cuda/_wrapper.py:1806-2002).
 
@@ -854,6 +877,15 @@ def rasterize_to_pixels_textured_gaussians(
     are staged in shared memory per batch (0: tile_size^2, the reference's).
     ``persistent=True`` launches as many CTAs as fit on the device, which take
     tiles from a device work counter instead of one CTA per tile.
+
+    ``transmittance``: "divide" (the reference's scheme: the adjoint recovers
+    each splat's transmittance by dividing the final one by (1 - alpha), back
+    to front over the whole list) or "checkpoint" (the forward also keeps
+    every pixel's transmittance at the end of each batch of its tile, and the
+    adjoint restarts the division from it at every batch, so rounding
+    accumulates over one batch instead of up to thousands of splats; closer to
+    exact arithmetic at pixels with many contributors, for a buffer of
+    (n_tiles + n_isects / batch_depth) x tile_size^2 floats).
     """
     _check_common(means2d, ray_transforms, colors, opacities, isect_offsets, tile_size, image_width, image_height,
                   backgrounds, packed, view_table)
@@ -884,7 +916,8 @@ def rasterize_to_pixels_textured_gaussians(
         float(texture_range_x), float(texture_range_y), int(image_width), int(image_height), int(tile_size),
         isect_offsets.contiguous(), flatten_ids.contiguous(), absgrad, gs_contrib_threshold, g_weight,
         _FILTER_ADJOINT[filtering], False, gaussian_ids, textures.shape[0],
-        _layout(tile_order, view_table, batch_depth, persistent, means2d.device), mip_levels, filter_code)
+        _layout(tile_order, view_table, batch_depth, persistent, means2d.device, transmittance), mip_levels,
+        filter_code)
     render_colors = out[0]
     if padded > 0:
         render_colors = render_colors[..., :-padded]

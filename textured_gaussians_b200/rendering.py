@@ -20,9 +20,12 @@ tiles taken by descending intersection count, so the longest tiles do not form
 the launch's tail; "launch": tile index order; the results are the same),
 ``batch_depth`` (splats staged per compositor batch; 0 = tile_size^2),
 ``persistent`` (compositor CTAs take tiles from a device work counter),
-``tile_size`` 32 besides the reference's 8 and 16, and ``fuse_sh`` (default
+``tile_size`` 32 besides the reference's 8 and 16, ``fuse_sh`` (default
 on: the SH colours are computed inside the projection kernels instead of the
-reference's separate SH op + camera-centre inverse + clamp glue).
+reference's separate SH op + camera-centre inverse + clamp glue), and, for
+the textured renderer, ``transmittance`` ("divide", the reference's scheme, or
+"checkpoint": per-batch transmittance kept by the forward, see
+``rasterize_to_pixels_textured_gaussians``).
 """
 from __future__ import annotations
 
@@ -251,6 +254,7 @@ def rasterization_textured_gaussians(
     batch_depth: int = 0,
     persistent: bool = False,
     fuse_sh: bool = True,
+    transmittance: str = "divide",
 ) -> Tuple[Tensor, Tensor, Tensor, Optional[Tensor], Tensor, Tensor, Tensor, Tensor, Dict]:
     """Rasterize textured 2D Gaussian surfels (reference: rendering.py:1342-1685).
 
@@ -270,5 +274,5 @@ def rasterization_textured_gaussians(
         gs_contrib_threshold=gs_contrib_threshold, filtering=filtering, g_weight=g_weight,
         texture_storage=texture_storage, texture_scales=texture_scales, gaussian_ids=p["gaussian_ids"],
         tile_order=p["tile_order"], batch_depth=batch_depth,
-        persistent=persistent)
+        persistent=persistent, transmittance=transmittance)
     return _finish(p, *outs, viewmats, Ks, width, height, tile_size, render_mode, depth_mode)
