@@ -43,6 +43,12 @@ def upstream(seed: int, s) -> list:
     return [rng.normal(size=sh).astype(np.float32) for sh in shapes]
 
 
+def proj_upstream(seed: int, C: int, N: int) -> list:
+    """Upstream gradients of the projection's means2d, depths, ray transforms and normals (the fixture's)."""
+    rng = np.random.default_rng(int(seed))
+    return [rng.normal(size=sh).astype(np.float32) for sh in ((C, N, 2), (C, N), (C, N, 3, 3), (C, N, 3))]
+
+
 def scene(case: str, g: dict):
     """The scene a small fixture was made from, verified against its input digest."""
     if case == "small":

@@ -97,6 +97,14 @@ def upstream(seed, shapes):
     return [rng.normal(size=s).astype(np.float32) for s in shapes]
 
 
+def proj_upstream(seed, cn):
+    """Upstream gradients of the projection's outputs means2d [C,N,2], depths [C,N], ray transforms
+    [C,N,3,3] and normals [C,N,3]."""
+    rng = np.random.default_rng(seed)
+    C, N = cn
+    return [rng.normal(size=sh).astype(np.float32) for sh in ((C, N, 2), (C, N), (C, N, 3, 3), (C, N, 3))]
+
+
 def keep_rows(v, n_keep, seed=0):
     """A deterministic subset of the nonzero rows of v [G, ...], and every row's L2 norm."""
     flat = v.reshape(v.shape[0], -1)
@@ -207,6 +215,18 @@ def small_case(R, W, s, filters):
         p = project_and_shade(W, s, means, quats, scales, colors)
     for k in ("radii", "means2d", "depths", "M", "normals", "colors", "tpg", "isect_ids", "flatten_ids", "offsets"):
         d[f"stage__{k}"] = npy(p[k])
+    # the projection's adjoint on its own (_wrapper.py:1267 fully_fused_projection_2dgs): seeded upstream
+    # gradients on every visible entry's outputs (culled entries' outputs are left unwritten by the reference)
+    pleaves = [x.detach().clone().requires_grad_(True) for x in (means, quats, scales)]
+    pr = W.fully_fused_projection_2dgs(*pleaves, T(s.viewmats), T(s.Ks), s.width, s.height, 0.3, s.near_plane,
+                                       s.far_plane, 0.0)
+    d["projvjp_seed"] = np.array(77)
+    pups = proj_upstream(77, pr[0].shape)
+    vis = (pr[0] > 0).float()
+    loss = sum((o * T(u) * vis.view(vis.shape + (1,) * (o.dim() - 2))).sum() for o, u in zip(pr[1:], pups))
+    loss.backward()
+    for k, leaf in zip(("means", "quats", "scales"), pleaves):
+        d[f"projvjp__v_{k}"] = npy(leaf.grad)
     seeds = {"up": 101}
     d["up_seed"] = np.array(seeds["up"])
     ups = upstream(seeds["up"], pixel_shapes(s))

@@ -123,8 +123,11 @@ __device__ __forceinline__ bool project_one(const float* __restrict__ means, con
     const f3 RS2 = mul(R, Rq.c2);
     const float* K = Ks + 9 * c;
     const float fx = __ldg(K + 0), cx = __ldg(K + 2), fy = __ldg(K + 4), cy = __ldg(K + 5);
-    const f3 M0 = mk3(fx * RS0.x + cx * RS0.z, fx * RS1.x + cx * RS1.z, fx * mc.x + cx * mc.z);
-    const f3 M1 = mk3(fy * RS0.y + cy * RS0.z, fy * RS1.y + cy * RS1.z, fy * mc.y + cy * mc.z);
+    // K applied to each column as the reference's (W H)^T K^T product accumulates it
+    // (fully_fused_projection_2dgs_fwd.cu:157): the fx / fy term first, then the cx / cy term fused onto
+    // it -- the same rounding, so the ray transforms equal the reference's bit for bit
+    const f3 M0 = mk3(__fmaf_rn(RS0.z, cx, RS0.x * fx), __fmaf_rn(RS1.z, cx, RS1.x * fx), __fmaf_rn(mc.z, cx, mc.x * fx));
+    const f3 M1 = mk3(__fmaf_rn(RS0.z, cy, RS0.y * fy), __fmaf_rn(RS1.z, cy, RS1.y * fy), __fmaf_rn(mc.z, cy, mc.y * fy));
     const f3 M2 = mk3(RS0.z, RS1.z, mc.z);
     const float distance = M2.x * M2.x + M2.y * M2.y - M2.z * M2.z;
     if (fabsf(distance) < kDegenerateRel * (M2.x * M2.x + M2.y * M2.y + M2.z * M2.z))
