@@ -992,9 +992,88 @@ def reference_cuda(args):
     return out
 
 
+def cpu_config_table():
+    """The CPU cost of the small workloads run whole, and of one camera of the views8 workload, on the host's
+    cores: the reference's own torch stages (projection, SH, intersection, offsets) plus the oracle's FP32
+    compositor forward + backward.  Printed by --impl reference --cpu-configs (one JSON line)."""
+    import torch
+
+    from oracle import oracle as O
+    from textured_gaussians_b200 import scenes
+
+    mods = reference_cpu()
+    ti, ti2 = mods if mods is not None else (None, None)
+    torch.set_num_threads(os.cpu_count() or 1)
+    rows = {}
+    for name, make in (("config0_small", scenes.small), ("config2_adjoint", scenes.adjoint),
+                       ("config1_views8_camera0", lambda: scenes.views8(with_textures=False))):
+        s = make()
+        V, K = s.viewmats[:1], s.Ks[:1]
+        N, W, H, ts = s.means.shape[0], s.width, s.height, s.tile_size
+        tw, th = -(-W // ts), -(-H // ts)
+        st = {}
+        if ti2 is not None:
+            means, quats, scales = (torch.from_numpy(x) for x in (s.means, s.quats, s.scales))
+            t0 = time.perf_counter()
+            radii_t, m2d_t, dep_t, _, _ = ti2._fully_fused_projection_2dgs(means, quats, scales, torch.from_numpy(V),
+                                                                          torch.from_numpy(K), W, H, s.near_plane,
+                                                                          s.far_plane)
+            st["ref_projection"] = time.perf_counter() - t0
+            cam = torch.linalg.inv(torch.from_numpy(V))[:, :3, 3]
+            t0 = time.perf_counter()
+            ti._spherical_harmonics(s.sh_degree, means[None] - cam[:, None], torch.from_numpy(s.colors)[None])
+            st["ref_sh"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            _, ids_t, _ = ti._isect_tiles(m2d_t, radii_t.int(), dep_t, ts, tw, th)
+            st["ref_isect"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            ti._isect_offset_encode(ids_t, 1, tw, th)
+            st["ref_offsets"] = time.perf_counter() - t0
+        radii, m2d, dep, M, nrm = O.project_fwd(s.means, s.quats, s.scales, V, K, W, H, s.near_plane, s.far_plane)
+        _, ids, fl = O.isect_tiles(m2d, radii, dep, ts, tw, th, 1)
+        off = O.isect_offset_encode(ids, 1, tw, th)
+        cam = np.linalg.inv(V.astype(np.float64))[:, :3, 3]
+        cols = np.maximum(O.sh_fwd(s.sh_degree, (s.means[None] - cam[:, None]).astype(np.float32), s.colors,
+                                   masks=radii > 0) + 0.5, 0).astype(np.float32)
+        R = s.textures.shape[1] if s.textures is not None else s.extra["texture_res"]
+        if s.textures is not None:
+            tex, gid, ng = s.textures, None, None
+        else:  # 12 GB of textures would not be reasonable on the host: one shared texture, the same work
+            tex, gid, ng = np.full((1, R, R, 4), 0.5, np.float32), np.zeros(N, np.int64), 1
+        args = (m2d, M, cols, s.opacities[None], nrm, tex, off, fl, W, H, ts)
+        kw = {} if gid is None else dict(gaussian_ids=gid, n_gauss=ng)
+        if gid is not None:
+            args = (m2d[0], M[0], cols[0], s.opacities, nrm[0]) + args[5:]
+        rng = np.random.default_rng(0)
+        up = [rng.normal(size=(1, H, W, c)).astype(np.float32) for c in (3, 1, 3, 1, 1)]
+        t0 = time.perf_counter()
+        fo = O.raster_fwd(*args, backgrounds=s.backgrounds, **kw)
+        O.raster_bwd(*args, fo, *up, backgrounds=s.backgrounds, **kw)
+        st["oracle_compositor_fwd_bwd"] = time.perf_counter() - t0
+        total = sum(st.values())
+        rows[name] = {"splats": N, "texture": f"{R}x{R}", "pixels": W * H, "tile": ts,
+                      "stage_s": {k: round(v, 4) for k, v in st.items()},
+                      "value": round(W * H / total / 1e6, 4), "unit": "Mpix/s"}
+    return {"cpu_configs": rows, "cores": os.cpu_count(), "cpu": _cpu_model()}
+
+
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return
+    if args.cpu_configs:
+        print(json.dumps(cpu_config_table()), flush=True)
         return
     samples = []
     for _ in range(args.warmup + args.steps):
@@ -1043,6 +1122,9 @@ def main():
     ap.add_argument("--views", type=int, default=64, help="views of the batch workload")
     ap.add_argument("--tile-order", default="heaviest_first", choices=["launch", "heaviest_first"],
                     help="compositor tile order of the headline form")
+    ap.add_argument("--cpu-configs", action="store_true",
+                    help="with --impl reference: time the small workloads whole on the CPU (reference torch stages "
+                         "+ oracle compositor) instead of the benchmark line")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes of one compositor-adjoint launch from an ncu capture, reported as roofline.traffic")
     args = ap.parse_args()
