@@ -418,6 +418,14 @@ typedef struct {
      * bs the batch depth (tile_size^2 when batch_depth is 0); row
      * t + tile_offsets[t] / bs + k holds batch k of tile t. */
     float* t_checkpoints;
+    /* TG_FILTER_ANISO_BILINEAR only: the row-prefix table of the textures,
+     * [G,ry,rx,4] FP32 as made by tg_aniso_prefix, or NULL.  When set, a
+     * footprint whose corner rays meet the splat plane on one side (a convex
+     * quad) is integrated along its boundary (Green's theorem over the rows'
+     * prefix integrals: work in proportion to its perimeter in texel cells)
+     * instead of cell by cell as the reference does; the same integral up to
+     * FP32 rounding.  No counterpart in the reference. */
+    const float* aniso_prefix;
 } tg_raster_fwd_args;
 TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
 
@@ -449,6 +457,10 @@ typedef struct {
     float* v_textures;           /* [G,ry,rx,4] FP32 or NULL */
     float* v_densify;            /* [E,2] */
     float* v_tex_coarse;         /* mipmapped2: [G, (4^L - 1) / 3, 4] gradient of tex_coarse (zeroed by the call) */
+    /* anisotropic_bilinear with f.aniso_prefix set and v_textures requested:
+     * [G,ry,rx,4] FP32 scratch for the gradient of the row-prefix table; the
+     * call zeroes it and folds it into v_textures after the accumulation. */
+    float* v_aniso_prefix;
 } tg_raster_bwd_args;
 TG_API int tg_rasterize_bwd(const tg_raster_bwd_args* a, tg_stream_t stream);
 
@@ -479,6 +491,16 @@ TG_API int tg_sh_bwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, c
  * 10, ... are modified when L > 5).  1 <= L <= 13. */
 TG_API int tg_generate_mipmap(const float* textures, float* coarse, int64_t G, int32_t L, tg_stream_t stream);
 TG_API int tg_generate_mipmap_bwd(float* v_coarse, float* v_textures, int64_t G, int32_t L, tg_stream_t stream);
+
+/* ------------------------------------------------------------------ anisotropic_bilinear row prefixes
+ * The table tg_raster_fwd_args.aniso_prefix points to: for texture g, row r
+ * and column u, prefix[g,r,u] = sum_{k<u} (t(g,r,k) + t(g,r,k+1)) / 2 (the
+ * integral of the row's linear interpolant from column 0 to u; 0 at u = 0),
+ * per channel, FP32 [G,ry,rx,4], decoded from `textures` in tex_format
+ * (TG_TEX_F32/BF16/F16/FP8_E4M3, tex_scales [G] for fp8).  Rebuild it
+ * whenever the textures change.  No counterpart in the reference. */
+TG_API int tg_aniso_prefix(const void* textures, int32_t tex_format, const float* tex_scales, int64_t G, int32_t ry,
+                           int32_t rx, float* prefix, tg_stream_t stream);
 
 /* ------------------------------------------------------------------ gradient consumers
  * Replaces selective_adam_update (textured_gaussians/cuda/csrc/adam.cu:17-89):

@@ -1,7 +1,9 @@
 """GPU parity of the anisotropic_bilinear filter: the compositor integrating
-each pixel's texture-space footprint quad cell by cell, forward and reference
-adjoint, against the CPU oracle (the reference's Sutherland-Hodgman clipping
-restated; the kernel sums the same clipped polygon's boundary piecewise).
+each pixel's texture-space footprint quad, forward and reference adjoint,
+against the CPU oracle (the reference's Sutherland-Hodgman clipping restated),
+with both integrations the compositor has: "cells" (cell by cell, each clipped
+polygon's boundary summed piecewise) and "boundary" (a convex footprint along
+its boundary over the textures' row-prefix tables, Green's theorem).
 
 Tolerances: the oracle evaluated in FP64 on the same FP32 inputs; 1e-5
 absolute per forward output with a 1e-3 fraction of branch flips (cell ranges
@@ -15,6 +17,8 @@ import pytest
 import torch
 
 from oracle import oracle as O
+from textured_gaussians_b200 import _backend as B
+from textured_gaussians_b200.cuda import _wrapper as W
 from tests._util import assert_close, rel_l2, to_np
 from textured_gaussians_b200 import rasterization_textured_gaussians, scenes
 from textured_gaussians_b200.cuda import (
@@ -28,6 +32,12 @@ from textured_gaussians_b200.cuda import (
 pytestmark = pytest.mark.gpu
 DEV = "cuda:0"
 F64 = np.float64
+
+
+@pytest.fixture(autouse=True, params=["boundary", "cells"])
+def integration(request, monkeypatch):
+    monkeypatch.setattr(W, "ANISO_INTEGRATION", request.param)
+    return request.param
 
 SCENES = {"tiny": lambda: scenes.tiny(), "tiny32": lambda: scenes.tiny(R=32),
           "tiny3cam": lambda: scenes.tiny(seed=7, n_cams=3), "small": lambda: scenes.small(),
@@ -159,3 +169,42 @@ def test_aniso_rejects_what_it_does_not_support():
     with pytest.raises(RuntimeError, match="FP32 and BF16"):
         rasterize_to_pixels_textured_gaussians(*args, filtering="anisotropic_bilinear", texture_storage=store,
                                                texture_scales=scales)
+
+
+@pytest.mark.parametrize("fmt", ["fp32", "bf16", "fp16", "fp8"])
+@pytest.mark.parametrize("ry,rx", [(32, 32), (3, 70), (5, 1), (1, 2)])
+def test_aniso_prefix_table_matches_the_rows_trapezoid_sums(fmt, ry, rx, integration):
+    if integration != "boundary":
+        pytest.skip("one run is enough")
+    rng = np.random.default_rng(ry * 100 + rx)
+    tex = T(rng.uniform(-1, 2, size=(37, ry, rx, 4)).astype(np.float32))
+    store, scales = make_texture_storage(tex, fmt)
+    st = torch.cuda.current_stream().cuda_stream
+    P = W._aniso_prefix(store, scales, st)
+    deq = store.float() if scales is None else store.float() * scales[:, None, None, None]
+    t = deq.double().cpu().numpy()
+    ref = np.zeros_like(t)
+    ref[:, :, 1:] = np.cumsum(0.5 * (t[:, :, :-1] + t[:, :, 1:]), axis=2)
+    got = P.cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-5 * max(1.0, np.abs(ref).max()), np.abs(got - ref).max()
+    assert np.all(got[:, :, 0] == 0)
+
+
+def test_aniso_boundary_and_cells_agree_on_a_large_scene(integration):
+    """Both integrations on one 1600x1200 view of a 150,000-splat mixture scene (32x32 textures)."""
+    if integration != "boundary":
+        pytest.skip("one run is enough")
+    s = scenes.mixture1m(N=150_000, n_cams=1)
+    outs = {}
+    for mode in ("cells", "boundary"):
+        W.ANISO_INTEGRATION = mode
+        d = _inputs(s, 8)
+        tex = d["tex"].detach().clone().requires_grad_()
+        out = rasterize_to_pixels_textured_gaussians(
+            d["means2d"], d["M"], T(d["colors"]), T(d["opac"]), tex, 3.0, 3.0, d["normals"],
+            torch.zeros_like(d["means2d"]), s.width, s.height, 8, d["off"], d["fl"], filtering="anisotropic_bilinear")
+        (out[0].sum() + out[1].sum()).backward()
+        outs[mode] = (to_np(out[0]), to_np(out[1]), to_np(tex.grad))
+    for i, name in enumerate(("colors", "alphas")):
+        assert_close(outs["boundary"][i], outs["cells"][i], 1e-5, 1e-5, 1e-3, name)
+    assert rel_l2(outs["boundary"][2], outs["cells"][2]) < 1e-4

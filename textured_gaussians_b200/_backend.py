@@ -81,7 +81,7 @@ class RasterFwdArgs(ctypes.Structure):
                 ("last_ids", P), ("median_ids", P), ("contrib_sum", P), ("contrib_count", P), ("tile_order", P),
                 ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64), ("n_isects_dev", P),
                 ("batch_depth", I32), ("work_queue", P), ("mip_levels", I32), ("tex_coarse", P),
-                ("filter", I32), ("t_checkpoints", P)]
+                ("filter", I32), ("t_checkpoints", P), ("aniso_prefix", P)]
 
 
 class RasterBwdArgs(ctypes.Structure):
@@ -89,7 +89,8 @@ class RasterBwdArgs(ctypes.Structure):
                 ("median_ids", P), ("v_render_colors", P), ("v_render_alphas", P), ("v_render_normals", P),
                 ("v_render_distort", P), ("v_render_median", P), ("adjoint", I32), ("n_elems", I64),
                 ("v_means2d", P), ("v_means2d_abs", P), ("v_ray_transforms", P), ("v_colors", P),
-                ("v_opacities", P), ("v_normals", P), ("v_textures", P), ("v_densify", P), ("v_tex_coarse", P)]
+                ("v_opacities", P), ("v_normals", P), ("v_textures", P), ("v_densify", P), ("v_tex_coarse", P),
+                ("v_aniso_prefix", P)]
 
 
 _lib = None
@@ -130,6 +131,7 @@ def lib() -> ctypes.CDLL:
                 ("tg_densify_stats", [ctypes.POINTER(DensifyStatsArgs), P]),
                 ("tg_generate_mipmap", [P, P, I64, I32, P]),
                 ("tg_generate_mipmap_bwd", [P, P, I64, I32, P]),
+                ("tg_aniso_prefix", [P, I32, P, I64, I32, I32, P, P]),
                 ("tg_sh_bwd", [I64, I64, I32, I32, P, P, P, P, P, P, P]),
             ]:
                 fn = getattr(L, name)

@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtg2dgs.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["capi.cu", "projection.cu", "isect.cu", "raster_fwd.cu", "raster_bwd.cu", "sh.cu", "sort_noalloc.cu", "optim.cu", "mip.cu"]
+SOURCES = ["capi.cu", "projection.cu", "isect.cu", "raster_fwd.cu", "raster_bwd.cu", "sh.cu", "sort_noalloc.cu", "optim.cu", "mip.cu", "aniso.cu"]
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "--use_fast_math", "-lineinfo", "-std=c++17",

@@ -46,6 +46,10 @@ cudaError_t launch_selective_adam(float* param, const float* grad, float* m, flo
 cudaError_t launch_densify_stats(const tg_densify_stats_args& a, cudaStream_t s);
 cudaError_t launch_generate_mipmap(const float* textures, float* coarse, int64_t G, int L, cudaStream_t s);
 cudaError_t launch_generate_mipmap_bwd(float* v_coarse, float* v_textures, int64_t G, int L, cudaStream_t s);
+cudaError_t launch_aniso_prefix(const void* textures, int tex_format, const float* tex_scales, int64_t G, int ry,
+                                int rx, float* prefix, cudaStream_t s);
+cudaError_t launch_aniso_prefix_fold(const float* v_prefix, int64_t G, int ry, int rx, float* v_textures,
+                                     cudaStream_t s);
 int fail_with(int code, const char* msg);
 }  // namespace tg
 
@@ -168,6 +172,8 @@ int check_raster_common(const tg_raster_fwd_args& a) {
         TG_REQUIRE(a.D == 3 || a.D == 4, TG_ERR_UNSUPPORTED, "the anisotropic_bilinear filter supports 3 or 4 channels");
         TG_REQUIRE(a.tile_size <= 16 && a.work_queue == nullptr, TG_ERR_UNSUPPORTED,
                    "the anisotropic_bilinear filter runs with tile 8 or 16 and one CTA per tile");
+        TG_REQUIRE(a.aniso_prefix == nullptr || aligned(a.aniso_prefix, 16), TG_ERR_INVALID_ARG,
+                   "aniso_prefix must be 16-byte aligned");
     }
     return TG_OK;
 }
@@ -436,6 +442,12 @@ int tg_rasterize_bwd(const tg_raster_bwd_args* a, tg_stream_t stream) {
     TG_REQUIRE(a->v_means2d && a->v_ray_transforms && a->v_colors && a->v_opacities && a->v_normals && a->v_densify,
                TG_ERR_INVALID_ARG, "null gradient output");
     if (a->v_textures) TG_REQUIRE(aligned(a->v_textures, 16), TG_ERR_INVALID_ARG, "v_textures must be 16-byte aligned");
+    // the boundary-integral adjoint accumulates the row-prefix gradient, folded into v_textures afterwards
+    const bool fold = a->f.filter == TG_FILTER_ANISO_BILINEAR && a->f.aniso_prefix != nullptr &&
+                      a->v_textures != nullptr;
+    if (fold)
+        TG_REQUIRE(a->v_aniso_prefix && aligned(a->v_aniso_prefix, 16), TG_ERR_INVALID_ARG,
+                   "anisotropic_bilinear with aniso_prefix needs a 16-byte aligned v_aniso_prefix");
     const int64_t E = a->n_elems;
     const int D = a->f.D;
     const size_t tex_bytes = a->f.tex_format == TG_TEX_NONE || a->v_textures == nullptr
@@ -449,13 +461,20 @@ int tg_rasterize_bwd(const tg_raster_bwd_args* a, tg_stream_t stream) {
         {a->v_tex_coarse, a->f.mip_levels > 0 && a->v_textures
                               ? sizeof(float) * 4 * (size_t)(((int64_t(1) << (2 * a->f.mip_levels)) - 1) / 3) *
                                     (size_t)a->f.n_contrib
-                              : 0}};
+                              : 0},
+        {fold ? a->v_aniso_prefix : nullptr, tex_bytes}};
     for (const Z& z : zs)
         if (z.p && z.n) {
             cudaError_t e = cudaMemsetAsync(z.p, 0, z.n, stream);
             if (e != cudaSuccess) return cuda_status(e, "tg_rasterize_bwd memset");
         }
-    return cuda_status(tg::launch_raster_bwd(*a, stream), "tg_rasterize_bwd");
+    tg_raster_bwd_args b = *a;
+    if (!fold) b.v_aniso_prefix = nullptr;
+    cudaError_t e = tg::launch_raster_bwd(b, stream);
+    if (e == cudaSuccess && fold)
+        e = tg::launch_aniso_prefix_fold(a->v_aniso_prefix, a->f.n_contrib, a->f.tex_ry, a->f.tex_rx, a->v_textures,
+                                         stream);
+    return cuda_status(e, "tg_rasterize_bwd");
 }
 
 int tg_sh_fwd(int64_t n, int64_t coeff_rows, int32_t degree, int32_t K, const float* dirs, const float* coeffs,
@@ -508,6 +527,21 @@ int tg_generate_mipmap_bwd(float* v_coarse, float* v_textures, int64_t G, int32_
     TG_REQUIRE(v_coarse && v_textures && aligned(v_coarse, 16) && aligned(v_textures, 16), TG_ERR_INVALID_ARG,
                "null or misaligned pointer");
     return cuda_status(tg::launch_generate_mipmap_bwd(v_coarse, v_textures, G, L, stream), "tg_generate_mipmap_bwd");
+}
+
+int tg_aniso_prefix(const void* textures, int32_t tex_format, const float* tex_scales, int64_t G, int32_t ry,
+                    int32_t rx, float* prefix, tg_stream_t stream) {
+    TG_REQUIRE(G >= 0 && ry >= 1 && rx >= 1, TG_ERR_INVALID_ARG, "bad sizes (G %lld, ry %d, rx %d)", (long long)G, ry,
+               rx);
+    TG_REQUIRE(tex_format == TG_TEX_F32 || tex_format == TG_TEX_BF16 || tex_format == TG_TEX_F16 ||
+                   tex_format == TG_TEX_FP8_E4M3,
+               TG_ERR_INVALID_ARG, "bad texture format %d", tex_format);
+    if (G == 0) return TG_OK;
+    TG_REQUIRE(textures && prefix && aligned(prefix, 16) && aligned(textures, tex_format == TG_TEX_F32 ? 16 : 8),
+               TG_ERR_INVALID_ARG, "null or misaligned pointer");
+    TG_REQUIRE(tex_format != TG_TEX_FP8_E4M3 || tex_scales != nullptr, TG_ERR_INVALID_ARG, "fp8 needs tex_scales");
+    return cuda_status(tg::launch_aniso_prefix(textures, tex_format, tex_scales, G, ry, rx, prefix, stream),
+                       "tg_aniso_prefix");
 }
 
 int tg_densify_stats(const tg_densify_stats_args* a, tg_stream_t stream) {

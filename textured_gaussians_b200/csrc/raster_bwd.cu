@@ -400,7 +400,9 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
                     const bool act = P[q].inside && idx <= P[q].bin_final && in_box(box, P[q].px, P[q].py);
                     PairOf<Filt> e;
                     eval_aniso_coop<Tex, true>(e, act, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx,
-                                         f.tex_ry, f.range_x, f.range_y, f.g_weight, wmask);
+                                         f.tex_ry, f.range_x, f.range_y, f.g_weight, wmask,
+                                         f.aniso_prefix ? reinterpret_cast<const float4*>(f.aniso_prefix) + tex_base
+                                                        : nullptr);
                     const bool use = act && e.valid;
                     float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (use) {
@@ -411,7 +413,9 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
                     aniso_coop_scatter<true>(e.F, g4,
                                        use && e.tex_valid && vt != nullptr &&
                                            (g4.x != 0.f || g4.y != 0.f || g4.z != 0.f || g4.w != 0.f),
-                                       vt, f.tex_rx, wmask);
+                                       vt, f.tex_rx, wmask,
+                                       a.v_aniso_prefix != nullptr ? a.v_aniso_prefix + 4 * tex_base : nullptr,
+                                       f.tex_ry);
                     continue;
                 }
                 if (!(P[q].inside && idx <= P[q].bin_final) || !in_box(box, P[q].px, P[q].py)) continue;

@@ -261,6 +261,229 @@ __device__ __forceinline__ float4 aniso_cell(const AnisoFoot& F, int u, int v) {
         return cell_edges_sum(F.s, F.r, u, v);
 }
 
+// ---------------------------------------------------------------- anisotropic_bilinear by boundary integral
+// The footprint integral of the bilinear interpolant f over P = quad ∩ [0, rx-1] x [0, ry-1] (the cells the
+// reference visits, clamped to the texture) is turned into a line integral by Green's theorem:
+//   ∫∫_P f dA = ∮_∂P F dy,   F(x, y) = ∫_{x0}^{x} f(s, y) ds   (∂P counter-clockwise, x0 = the first cell column),
+// and F is read from per-row prefix integrals of the texture (the rows' trapezoid sums,
+// P_r[u] = Σ_{k<u} (t(k,r) + t(k+1,r)) / 2, built once per call by tg_aniso_prefix):
+//   F = (1 - y') (P_v[u] - P_v[x0] + a (x' - x'²/2) + b x'²/2) + y' (P_{v+1}[u] - P_{v+1}[x0] + c (x' - x'²/2) + d x'²/2)
+// in cell (u, v) with texels a, b, c, d = t(u,v), t(u+1,v), t(u,v+1), t(u+1,v+1) and x' = x - u, y' = y - v.
+// Along a straight piece inside one cell F is a cubic in the line parameter, so two-point Gauss-Legendre is
+// exact.  The boundary is the quad's four edges clipped to the texture box plus the box's right edge
+// x = rx - 1 where the quad reaches past it (on the left edge x = x0 = 0 F vanishes; the top and bottom
+// edges have dy = 0).  Work per footprint is proportional to its perimeter in cells, not its area.  Only
+// convex footprints take this route; the others keep the reference's per-cell polygon clipping.
+
+// Weights of one piece a -> b of the boundary inside cell (u, v): the piece's integral is
+//   wa a + wb b + wc c + wd d + wp0 (P_v[u] - P_v[x0]) + wp1 (P_{v+1}[u] - P_{v+1}[x0]).
+struct PieceW {
+    float wa, wb, wc, wd, wp0, wp1;
+};
+__device__ __forceinline__ PieceW piece_weights(float2 a, float2 b, int u, int v) {
+    constexpr float kG = 0.21132486540518713f;  // (1 - 1/sqrt(3)) / 2: the Gauss points are kG and 1 - kG
+    const float dx = b.x - a.x, dy = b.y - a.y;
+    PieceW w{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const float tq = q == 0 ? kG : 1.f - kG;
+        const float x = (a.x - (float)u) + tq * dx, y = (a.y - (float)v) + tq * dy;
+        const float x2 = 0.5f * x * x, x1 = x - x2;
+        w.wa += (1.f - y) * x1;
+        w.wb += (1.f - y) * x2;
+        w.wc += y * x1;
+        w.wd += y * x2;
+        w.wp0 += 1.f - y;
+        w.wp1 += y;
+    }
+    const float h = 0.5f * dy;  // the two Gauss weights (1/2 each) times the piece's dy
+    w.wa *= h; w.wb *= h; w.wc *= h; w.wd *= h; w.wp0 *= h; w.wp1 *= h;
+    return w;
+}
+
+// Walks the segment a -> b through the texel cells it crosses (cells clamped to [0, rx-2] x [0, ry-2]) and
+// calls visit(piece start, piece end, u, v) for each piece with dy != 0.
+template <class Visit>
+__device__ __forceinline__ void walk_cells(float2 a, float2 b, int rx, int ry, Visit&& visit) {
+    const float dx = b.x - a.x, dy = b.y - a.y;
+    if (dy == 0.f) return;  // nothing to integrate along a horizontal piece
+    // starting cell: the one the segment enters from a (ties at a grid line go the way it heads)
+    int ix = dx >= 0.f ? (int)floorf(a.x) : (int)ceilf(a.x) - 1;
+    int iy = dy >= 0.f ? (int)floorf(a.y) : (int)ceilf(a.y) - 1;
+    const int sx = dx > 0.f ? 1 : (dx < 0.f ? -1 : 0), sy = dy > 0.f ? 1 : -1;
+    const float rdx = dx != 0.f ? 1.f / dx : 0.f, rdy = 1.f / dy;
+    float t = 0.f;
+    float2 p = a;
+    const int limit = 2 * (rx + ry) + 8;  // cells a clipped segment can cross, with margin
+    for (int it = 0; it < limit; ++it) {
+        const float tx = sx == 0 ? INFINITY : ((float)(sx > 0 ? ix + 1 : ix) - a.x) * rdx;
+        const float ty = ((float)(sy > 0 ? iy + 1 : iy) - a.y) * rdy;
+        const float tn = fminf(fminf(tx, ty), 1.f);
+        const float2 q = tn >= 1.f ? b : make_float2(a.x + tn * dx, a.y + tn * dy);
+        if (tn > t) visit(p, q, min(max(ix, 0), rx - 2), min(max(iy, 0), ry - 2));
+        if (tn >= 1.f) break;
+        if (tx <= tn) ix += sx;
+        if (ty <= tn) iy += sy;
+        t = tn;
+        p = q;
+    }
+}
+
+// The boundary of a convex footprint clipped to the texture box [0, rx-1] x [0, ry-1]: its corners s
+// (counter-clockwise), their edges' reciprocal components r, and its cell range.
+struct FootQuad {
+    float2 s[4], r[4];
+    int minu, maxu, minv, maxv;
+};
+
+// Visits every boundary piece of the footprint: the quad's four edges clipped to the box, then the box's
+// right edge inside the quad.  The five segments are clipped first; one walk then takes them in turn, so
+// the visitor's code exists once.
+template <class Visit>
+__device__ __forceinline__ void foot_boundary(const FootQuad& F, int rx, int ry, Visit&& visit) {
+    const float X1 = (float)(rx - 1), Y1 = (float)(ry - 1);
+    float2 sa[5], sb[5];
+    bool sk[5];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {  // the quad's edges inside the box
+        const float2 a = F.s[i], d = sub2(F.s[(i + 1) & 3], F.s[i]), r = F.r[i];
+        float t0 = 0.f, t1 = 1.f;
+        const bool k0 = clip_t(a.x, d.x, r.x, t0, t1), k1 = clip_t(X1 - a.x, -d.x, -r.x, t0, t1);
+        const bool k2 = clip_t(a.y, d.y, r.y, t0, t1), k3 = clip_t(Y1 - a.y, -d.y, -r.y, t0, t1);
+        sk[i] = k0 & k1 & k2 & k3 & (t0 < t1);
+        sa[i] = make_float2(a.x + t0 * d.x, a.y + t0 * d.y);
+        sb[i] = make_float2(a.x + t1 * d.x, a.y + t1 * d.y);
+    }
+    // the box's right edge x = X1 inside the quad, upward (counter-clockwise for the box): the segment
+    // (X1, 0) -> (X1, Y1) clipped against the quad's four half-planes cross(e_i, p - s_i) >= 0
+    {
+        float t0 = 0.f, t1 = 1.f;
+        bool keep = true;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 e = sub2(F.s[(i + 1) & 3], F.s[i]);
+            // cross(e, (X1, t Y1) - s_i) = cross(e, (X1, 0) - s_i) + t Y1 e.x
+            const float p = e.x * (0.f - F.s[i].y) - e.y * (X1 - F.s[i].x), q = e.x * Y1;
+            const bool k = clip_t(p, q, q != 0.f ? 1.f / q : 0.f, t0, t1);
+            // a quad edge on the line x = X1: the box edge is kept if the quad lies beyond it, or on it running
+            // downward (the two cancel); running upward the quad edge itself is the boundary, counted once
+            keep = keep & (q == 0.f ? (p > 0.f || (p == 0.f && e.y < 0.f)) : k);
+        }
+        sk[4] = keep && t0 < t1;
+        sa[4] = make_float2(X1, t0 * Y1);
+        sb[4] = make_float2(X1, t1 * Y1);
+    }
+#pragma unroll 1
+    for (int i = 0; i < 5; ++i) {
+        if (sk[0]) walk_cells(sa[0], sb[0], rx, ry, visit);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {  // next segment into slot 0 (static indices: the arrays stay in registers)
+            sa[j] = sa[j + 1];
+            sb[j] = sb[j + 1];
+            sk[j] = sk[j + 1];
+        }
+    }
+}
+
+// The footprint integral (before the division by the area) of a convex footprint, from the texture and its
+// row-prefix table P (the splat's [ry, rx] float4 rows).  (Gathering the weights per cell to read each texel
+// once, as the adjoint's scatter does for its atomics, measured 1.6x slower here: the loads hit L1.)
+template <class Tex>
+__device__ __forceinline__ float4 aniso_boundary_sum_impl(const FootQuad& F, const void* textures, int64_t tex_base,
+                                                          const float4* P, int rx, int ry, float scale) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!(F.maxu > F.minu && F.maxv > F.minv)) return acc;  // no cell (also: rx or ry below 2)
+    const int x0 = F.minu;
+    foot_boundary(F, rx, ry, [&](float2 a, float2 b, int u, int v) {
+        const PieceW w = piece_weights(a, b, u, v);
+        const int64_t t00 = tex_base + (int64_t)v * rx + u;
+        const float4 ta = Tex::load(textures, t00, scale), tb = Tex::load(textures, t00 + 1, scale);
+        const float4 tc = Tex::load(textures, t00 + rx, scale), td = Tex::load(textures, t00 + rx + 1, scale);
+        float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
+        if (u != x0) {
+            const float4 a0 = __ldg(P + (int64_t)v * rx + u), b0 = __ldg(P + (int64_t)v * rx + x0);
+            const float4 a1 = __ldg(P + (int64_t)(v + 1) * rx + u), b1 = __ldg(P + (int64_t)(v + 1) * rx + x0);
+            p0 = make_float4(a0.x - b0.x, a0.y - b0.y, a0.z - b0.z, a0.w - b0.w);
+            p1 = make_float4(a1.x - b1.x, a1.y - b1.y, a1.z - b1.z, a1.w - b1.w);
+        }
+        acc.x += w.wa * ta.x + w.wb * tb.x + w.wc * tc.x + w.wd * td.x + w.wp0 * p0.x + w.wp1 * p1.x;
+        acc.y += w.wa * ta.y + w.wb * tb.y + w.wc * tc.y + w.wd * td.y + w.wp0 * p0.y + w.wp1 * p1.y;
+        acc.z += w.wa * ta.z + w.wb * tb.z + w.wc * tc.z + w.wd * td.z + w.wp0 * p0.z + w.wp1 * p1.z;
+        acc.w += w.wa * ta.w + w.wb * tb.w + w.wc * tc.w + w.wd * td.w + w.wp0 * p0.w + w.wp1 * p1.w;
+    });
+    return acc;
+}
+
+// The same sum as one out-of-line copy, for the adjoint (which also has the scatter's walk: both inlined
+// outgrow the instruction cache).
+template <class Tex>
+static __device__ __noinline__ float4 aniso_boundary_sum_shared(const FootQuad F, const void* textures,
+                                                                int64_t tex_base, const float4* P, int rx, int ry,
+                                                                float scale) {
+    return aniso_boundary_sum_impl<Tex>(F, textures, tex_base, P, rx, ry, scale);
+}
+
+// Adjoint of aniso_boundary_sum for the gradient g (already divided by the area): texel gradients into vt
+// (the splat's [ry, rx] float4 rows) and row-prefix gradients into vP, which tg_rasterize_bwd folds back
+// into the texels afterwards.  The x0 terms of the sum are left out here: they integrate a function of y
+// alone around the closed boundary, which is zero, so the gradient is the same without them (and the
+// column x0 would take an atomic from every piece).  Weights of the cell being walked are kept in registers
+// and flushed when the walk leaves it; the two texels (and one prefix entry) a cell shares with the next
+// one along the walk carry over, so a piece costs about two texel atomics and one prefix atomic.
+static __device__ __noinline__ void aniso_boundary_scatter(const FootQuad F, float4 g, float* vt, float* vP, int rx,
+                                                           int ry) {
+    if (!(F.maxu > F.minu && F.maxv > F.minv)) return;
+    float4* T4 = reinterpret_cast<float4*>(vt);
+    float4* P4 = reinterpret_cast<float4*>(vP);
+    auto put = [&](float4* base, int64_t i, float w) {
+        if (w != 0.f) atomicAdd(base + i, make_float4(g.x * w, g.y * w, g.z * w, g.w * w));
+    };
+    auto flush = [&](int u, int v, float wa, float wb, float wc, float wd, float w0, float w1) {
+        const int64_t t00 = (int64_t)v * rx + u;
+        put(T4, t00, wa);
+        put(T4, t00 + 1, wb);
+        put(T4, t00 + rx, wc);
+        put(T4, t00 + rx + 1, wd);
+        put(P4, t00, w0);
+        put(P4, t00 + rx, w1);
+    };
+    int cu = -1, cv = -1;
+    float wa = 0.f, wb = 0.f, wc = 0.f, wd = 0.f, w0 = 0.f, w1 = 0.f;  // the current cell's pending weights
+    foot_boundary(F, rx, ry, [&](float2 a, float2 b, int u, int v) {
+        if (u != cu || v != cv) {
+            float na = 0.f, nb = 0.f, nc = 0.f, nd = 0.f, n0 = 0.f, n1 = 0.f;
+            if (cu >= 0) {
+                // texels and prefix entries shared with the next cell move over; the rest are flushed
+                if (v == cv && u == cu + 1) { na = wb; nc = wd; wb = wd = 0.f; }
+                else if (v == cv && u == cu - 1) { nb = wa; nd = wc; wa = wc = 0.f; }
+                else if (u == cu && v == cv + 1) { na = wc; nb = wd; n0 = w1; wc = wd = w1 = 0.f; }
+                else if (u == cu && v == cv - 1) { nc = wa; nd = wb; n1 = w0; wa = wb = w0 = 0.f; }
+                flush(cu, cv, wa, wb, wc, wd, w0, w1);
+            }
+            cu = u;
+            cv = v;
+            wa = na; wb = nb; wc = nc; wd = nd; w0 = n0; w1 = n1;
+        }
+        const PieceW w = piece_weights(a, b, u, v);
+        wa += w.wa; wb += w.wb; wc += w.wc; wd += w.wd; w0 += w.wp0; w1 += w.wp1;
+    });
+    if (cu >= 0) flush(cu, cv, wa, wb, wc, wd, w0, w1);
+}
+
+__device__ __forceinline__ FootQuad foot_quad(const AnisoFoot& F) {
+    FootQuad Q;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        Q.s[i] = F.s[i];
+        Q.r[i] = F.r[i];
+    }
+    Q.minu = F.minu;
+    Q.maxu = F.maxu;
+    Q.minv = F.minv;
+    Q.maxv = F.maxv;
+    return Q;
+}
+
 // Bilinear weights of a cell's four texels (u,v), (u+1,v), (u,v+1), (u+1,v+1) from its moments.
 __device__ __forceinline__ float4 cell_weights(float4 mo) {
     return make_float4(((mo.x - mo.y) - mo.z) + mo.w, mo.y - mo.w, mo.z - mo.w, mo.w);
@@ -524,9 +747,19 @@ __device__ __forceinline__ void foot_cell(const AnisoFoot& F, int i, int& u, int
 // The warp must be full (mask = all 32 lanes).
 template <class Tex, bool kShared = false>
 __device__ __forceinline__ float4 aniso_coop_sum(const AnisoFoot& Fown, bool need, const void* textures,
-                                                 int64_t tex_base, int rx, float scale, unsigned mask) {
+                                                 int64_t tex_base, int rx, float scale, unsigned mask,
+                                                 const float4* P = nullptr, int ry = 0) {
     const int lane = threadIdx.x & 31;
     float4 mine = make_float4(0.f, 0.f, 0.f, 0.f);
+    // with the row-prefix table, each lane integrates its own convex footprint along its boundary; the warp
+    // integrates the others together, cell by cell
+    if (P != nullptr && need && Fown.convex) {
+        if constexpr (kShared)
+            mine = aniso_boundary_sum_shared<Tex>(foot_quad(Fown), textures, tex_base, P, rx, ry, scale);
+        else
+            mine = aniso_boundary_sum_impl<Tex>(foot_quad(Fown), textures, tex_base, P, rx, ry, scale);
+        need = false;
+    }
     unsigned pending = __ballot_sync(mask, need);
     while (pending) {
         const int L = __ffs(pending) - 1;
@@ -559,8 +792,12 @@ __device__ __forceinline__ float4 aniso_coop_sum(const AnisoFoot& Fown, bool nee
 // already divided by the area; need: it has one), cells spread over the warp.
 template <bool kShared = false>
 __device__ __forceinline__ void aniso_coop_scatter(const AnisoFoot& Fown, float4 gown, bool need, float* vt, int rx,
-                                                   unsigned mask) {
+                                                   unsigned mask, float* vP = nullptr, int ry = 0) {
     const int lane = threadIdx.x & 31;
+    if (vP != nullptr && need && Fown.convex) {
+        aniso_boundary_scatter(foot_quad(Fown), gown, vt, vP, rx, ry);
+        need = false;
+    }
     unsigned pending = __ballot_sync(mask, need);
     while (pending) {
         const int L = __ffs(pending) - 1;
@@ -592,14 +829,15 @@ template <class Tex, bool kShared = false>
 __device__ __forceinline__ void eval_aniso_coop(PairEvalAniso& e, bool act, float px, float py, const float4 xyo,
                                                 const float4 m0, const float4 m1, const float4 m2,
                                                 const void* textures, int64_t tex_base, int rx, int ry, float range_x,
-                                                float range_y, float g_weight, unsigned mask) {
+                                                float range_y, float g_weight, unsigned mask,
+                                                const float4* P = nullptr) {
     e.valid = false;
     e.need = false;
     e.tex_valid = false;
     if (act)
         eval_pair<Tex, FiltAniso>(e, px, py, xyo, m0, m1, m2, textures, tex_base, rx, ry, range_x, range_y, g_weight);
     const bool need = act && e.valid && e.need;
-    const float4 ts = aniso_coop_sum<Tex, kShared>(e.F, need, textures, tex_base, rx, xyo.w, mask);
+    const float4 ts = aniso_coop_sum<Tex, kShared>(e.F, need, textures, tex_base, rx, xyo.w, mask, P, ry);
     if (!(act && e.valid)) return;
     e.asf = 0.f;
     if (need) {

@@ -171,7 +171,9 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
                 PairOf<Filt> e;
                 if constexpr (Filt::kAniso) {  // every lane takes part: the warp integrates footprints together
                     eval_aniso_coop<Tex>(e, act, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx,
-                                         a.tex_ry, a.range_x, a.range_y, a.g_weight, wmask);
+                                         a.tex_ry, a.range_x, a.range_y, a.g_weight, wmask,
+                                         a.aniso_prefix ? reinterpret_cast<const float4*>(a.aniso_prefix) + tex_base
+                                                        : nullptr);
                     if (!act) continue;
                 } else {
                     if (!act) continue;

@@ -614,6 +614,25 @@ def generate_mipmap(textures: Tensor, log_texture_res: int, log_reduce: int = 4,
     return _GenerateMipmap.apply(textures, int(log_texture_res))
 
 
+# How the anisotropic_bilinear filter integrates a footprint: "boundary" (a convex footprint along its
+# boundary, over row-prefix tables built per call by tg_aniso_prefix; the others cell by cell) or "cells"
+# (every footprint cell by cell, as the reference does).  The same integral up to FP32 rounding.
+ANISO_INTEGRATION = "boundary"
+
+
+def _aniso_prefix(tex_store, tex_scales, st):
+    """Row-prefix table [G, ry, rx, 4] FP32 of the texture storage (tg_aniso_prefix), or None."""
+    if tex_store is None or ANISO_INTEGRATION == "cells":
+        return None
+    if ANISO_INTEGRATION != "boundary":
+        raise ValueError(f"ANISO_INTEGRATION must be 'boundary' or 'cells', got {ANISO_INTEGRATION!r}")
+    G, ry, rx = tex_store.shape[:3]
+    prefix = torch.empty((G, ry, rx, 4), dtype=torch.float32, device=tex_store.device)
+    B.call("tg_aniso_prefix", st, B.lib().tg_aniso_prefix, B.ptr(tex_store), _tex_format(tex_store),
+           B.ptr(tex_scales), G, ry, rx, B.ptr(prefix), st)
+    return prefix
+
+
 def _fwd_args(means2d, ray_transforms, colors, opacities, normals, textures_store, tex_scales, range_x, range_y,
               backgrounds, masks, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
               gs_contrib_threshold, g_weight, C, N, layout=None, n_isects_dev=None, mip_levels=0, tex_coarse=None,
@@ -692,6 +711,8 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         ckpt = _checkpoint_buffer(layout, isect_offsets, flatten_ids, tile_size, C, dev)
         a.t_checkpoints = B.ptr(ckpt)
         st = B.stream_of(means2d)
+        prefix = _aniso_prefix(tex_store, tex_scales, st) if filter_code == B.TG_FILTER_ANISO_BILINEAR else None
+        a.aniso_prefix = B.ptr(prefix)
         B.call("tg_rasterize_fwd", st, B.lib().tg_rasterize_fwd, ctypes.byref(a), st)
         ctx.save_for_backward(means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, m,
                               tex_store, tex_scales, isect_offsets, flatten_ids, render_colors, render_alphas,
@@ -702,6 +723,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         ctx.n_isects_dev = n_dev
         ctx.mip = (mip_levels, coarse, filter_code)
         ctx.t_checkpoints = ckpt
+        ctx.aniso_prefix = prefix
         ctx.mark_non_differentiable(contrib_sum, contrib_count)
         return render_colors, render_alphas, render_normals, render_distort, render_median, contrib_sum, contrib_count
 
@@ -728,6 +750,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
                       backgrounds, m, width, height, tile_size, isect_offsets, flatten_ids, gaussian_ids, n_contrib,
                       0.0, g_weight, C, N, ctx.layout, ctx.n_isects_dev, *ctx.mip)
         f.t_checkpoints = B.ptr(ctx.t_checkpoints)
+        f.aniso_prefix = B.ptr(ctx.aniso_prefix)
         v_means2d = torch.empty_like(means2d)
         v_means2d_abs = torch.empty_like(means2d) if absgrad else None
         v_ray_transforms = torch.empty_like(ray_transforms)
@@ -745,6 +768,8 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         L = ctx.mip[0]
         v_coarse = torch.empty_like(ctx.mip[1]) if L and want_tex else None
         a.v_tex_coarse = B.ptr(v_coarse)
+        v_prefix = torch.empty_like(ctx.aniso_prefix) if ctx.aniso_prefix is not None and want_tex else None
+        a.v_aniso_prefix = B.ptr(v_prefix)
         st = B.stream_of(means2d)
         B.call("tg_rasterize_bwd", st, B.lib().tg_rasterize_bwd, ctypes.byref(a), st)
         if v_coarse is not None:
