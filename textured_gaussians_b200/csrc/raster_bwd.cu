@@ -263,6 +263,9 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
     int* s_row = reinterpret_cast<int*>(s_col + bs * D);
     int* s_g = s_row + bs;
     float* s_grad = reinterpret_cast<float*>(s_g + bs);  // [bs][NV]
+    // anisotropic_bilinear: the boundary integration's per-warp area (16-byte aligned: bs is a multiple of 32)
+    float4* s_aniso = Filt::kAniso ? reinterpret_cast<float4*>(s_grad + bs * NV) + (threadIdx.x >> 5) * kAnisoWarpF4
+                                   : nullptr;
     __shared__ int s_max_bin;
 
     const unsigned wmask = __activemask();
@@ -402,7 +405,8 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
                     eval_aniso_coop<Tex, true>(e, act, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx,
                                          f.tex_ry, f.range_x, f.range_y, f.g_weight, wmask,
                                          f.aniso_prefix ? reinterpret_cast<const float4*>(f.aniso_prefix) + tex_base
-                                                        : nullptr);
+                                                        : nullptr,
+                                         s_aniso);
                     const bool use = act && e.valid;
                     float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (use) {
@@ -415,7 +419,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
                                            (g4.x != 0.f || g4.y != 0.f || g4.z != 0.f || g4.w != 0.f),
                                        vt, f.tex_rx, wmask,
                                        a.v_aniso_prefix != nullptr ? a.v_aniso_prefix + 4 * tex_base : nullptr,
-                                       f.tex_ry);
+                                       f.tex_ry, s_aniso);
                     continue;
                 }
                 if (!(P[q].inside && idx <= P[q].bin_final) || !in_box(box, P[q].px, P[q].py)) continue;
@@ -511,11 +515,12 @@ cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     const tg_raster_fwd_args& f = a.f;
     const int tile_px = f.tile_size * f.tile_size;
     const int bs = f.batch_depth > 0 ? f.batch_depth : tile_px;
-    const size_t smem = bwd_smem_bytes(D, bs);
+    size_t smem = bwd_smem_bytes(D, bs);
     const int64_t blocks = f.views ? f.n_tiles : (int64_t)f.C * f.tile_width * f.tile_height;
     const float uv_scale = a.adjoint == TG_ADJ_BWD2 ? 1.f : (a.adjoint == TG_ADJ_EXACT ? 0.5f : 0.f);
     // mipmapped2 / anisotropic_bilinear: one pixel per thread, one CTA per tile
     const bool mip = f.mip_levels > 0, aniso = f.filter == TG_FILTER_ANISO_BILINEAR;
+    if (aniso) smem += (size_t)(tile_px / 32) * kAnisoWarpF4 * 16;  // the boundary integration's per-warp area
     if ((mip || aniso) && !filter_instance<D, Tex, FiltMip2>()) return cudaErrorInvalidValue;
     const bool four = tile_px > 256;  // 32x32 tiles: four pixels per thread, 256 threads
     const bool pers = f.work_queue != nullptr;

@@ -56,7 +56,7 @@ using PairEval = PairEvalT<4>;
 // 1 / area; tsum is the texture integral before the division by the area.
 struct AnisoFoot {
     float2 s[4], n[4];
-    float2 r[4];  // 1 / x and 1 / y of edge i, s[i+1] - s[i] (the clip divisors; unused where a component is 0)
+    float2 r[4];  // 1 / x and 1 / y of edge i, s[i+1] - s[i] (the cell clip divisors; unused where a component is 0)
     float nmax[4];
     int minu, maxu, minv, maxv;
     float iarea;
@@ -76,10 +76,11 @@ template <class Filt> using PairOf = typename PairOfT<Filt>::type;
 __device__ __forceinline__ float cross2(float2 a, float2 b) { return a.x * b.y - a.y * b.x; }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 
-// Orientation (counter-clockwise), texel-cell range, edge normals and margins
-// of the footprint quad; returns its area (precompute,
-// filters/anisotropic_bilinear.cuh:193-245).  Clears F.convex for a quad with
-// a zero-length edge.
+// Orientation (counter-clockwise) and texel-cell range of the footprint quad;
+// returns its area (precompute, filters/anisotropic_bilinear.cuh:193-245).
+// Clears F.convex for a quad with a zero-length edge.  What only the
+// cell-by-cell integration needs (edge reciprocals, normals, margins) is
+// aniso_cells_setup's.
 __device__ __forceinline__ float aniso_setup(AnisoFoot& F, int rx, int ry) {
     float area = 0.5f * (cross2(sub2(F.s[1], F.s[0]), sub2(F.s[2], F.s[1])) +
                          cross2(sub2(F.s[3], F.s[2]), sub2(F.s[0], F.s[3])));
@@ -89,19 +90,29 @@ __device__ __forceinline__ float aniso_setup(AnisoFoot& F, int rx, int ry) {
         F.s[1] = F.s[3];
         F.s[3] = t;
     }
-    float2 e[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        e[i] = sub2(F.s[(i + 1) & 3], F.s[i]);
-        F.r[i] = make_float2(__frcp_rn(e[i].x), __frcp_rn(e[i].y));
+        const float2 e = sub2(F.s[(i + 1) & 3], F.s[i]);
         // a zero-length edge (collapsed corner) has no half-plane: the polygon clipping handles that quad
-        if (e[i].x == 0.f && e[i].y == 0.f) F.convex = false;
+        if (e.x == 0.f && e.y == 0.f) F.convex = false;
     }
     // float -> int conversions saturate (NaN -> 0), so the cell range stays within the texture
     F.minu = max(0, (int)floorf(fminf(fminf(F.s[0].x, F.s[1].x), fminf(F.s[2].x, F.s[3].x))));
     F.maxu = min(rx - 1, (int)ceilf(fmaxf(fmaxf(F.s[0].x, F.s[1].x), fmaxf(F.s[2].x, F.s[3].x))));
     F.minv = max(0, (int)floorf(fminf(fminf(F.s[0].y, F.s[1].y), fminf(F.s[2].y, F.s[3].y))));
     F.maxv = min(ry - 1, (int)ceilf(fmaxf(fmaxf(F.s[0].y, F.s[1].y), fmaxf(F.s[2].y, F.s[3].y))));
+    return area;
+}
+
+// Edge reciprocals, normals and margins of the (oriented) footprint quad, for the cell-by-cell integration
+// (filters/anisotropic_bilinear.cuh:193-245).
+__device__ __forceinline__ void aniso_cells_setup(AnisoFoot& F) {
+    float2 e[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        e[i] = sub2(F.s[(i + 1) & 3], F.s[i]);
+        F.r[i] = make_float2(__frcp_rn(e[i].x), __frcp_rn(e[i].y));
+    }
     const float cx = (((F.s[0].x + F.s[1].x) + F.s[2].x) + F.s[3].x) * 0.25f;
     const float cy = (((F.s[0].y + F.s[1].y) + F.s[2].y) + F.s[3].y) * 0.25f;
 #pragma unroll
@@ -113,7 +124,6 @@ __device__ __forceinline__ float aniso_setup(AnisoFoot& F, int rx, int ry) {
         F.n[i] = n;
         F.nmax[i] = fmaxf(fabsf(n.x * 0.5f + n.y * 0.5f), fabsf(n.x * 0.5f - n.y * 0.5f));
     }
-    return area;
 }
 
 // Green's-theorem terms of one directed boundary segment a -> b (cell-local
@@ -329,24 +339,15 @@ __device__ __forceinline__ void walk_cells(float2 a, float2 b, int rx, int ry, V
     }
 }
 
-// The boundary of a convex footprint clipped to the texture box [0, rx-1] x [0, ry-1]: its corners s
-// (counter-clockwise), their edges' reciprocal components r, and its cell range.
-struct FootQuad {
-    float2 s[4], r[4];
-    int minu, maxu, minv, maxv;
-};
-
-// Visits every boundary piece of the footprint: the quad's four edges clipped to the box, then the box's
-// right edge inside the quad.  The five segments are clipped first; one walk then takes them in turn, so
-// the visitor's code exists once.
-template <class Visit>
-__device__ __forceinline__ void foot_boundary(const FootQuad& F, int rx, int ry, Visit&& visit) {
+// Clips the boundary of a convex footprint F to the texture box [0, rx-1] x [0, ry-1]: segments 0..3 are the
+// quad's edges inside the box, segment 4 the box's right edge inside the quad; sk[i]: segment i is kept.
+__device__ __forceinline__ void foot_segments(const AnisoFoot& F, int rx, int ry, float2 (&sa)[5], float2 (&sb)[5],
+                                              bool (&sk)[5]) {
     const float X1 = (float)(rx - 1), Y1 = (float)(ry - 1);
-    float2 sa[5], sb[5];
-    bool sk[5];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {  // the quad's edges inside the box
-        const float2 a = F.s[i], d = sub2(F.s[(i + 1) & 3], F.s[i]), r = F.r[i];
+        const float2 a = F.s[i], d = sub2(F.s[(i + 1) & 3], F.s[i]);
+        const float2 r = make_float2(1.f / d.x, 1.f / d.y);  // unused where a component is 0 (see clip_t)
         float t0 = 0.f, t1 = 1.f;
         const bool k0 = clip_t(a.x, d.x, r.x, t0, t1), k1 = clip_t(X1 - a.x, -d.x, -r.x, t0, t1);
         const bool k2 = clip_t(a.y, d.y, r.y, t0, t1), k3 = clip_t(Y1 - a.y, -d.y, -r.y, t0, t1);
@@ -356,46 +357,33 @@ __device__ __forceinline__ void foot_boundary(const FootQuad& F, int rx, int ry,
     }
     // the box's right edge x = X1 inside the quad, upward (counter-clockwise for the box): the segment
     // (X1, 0) -> (X1, Y1) clipped against the quad's four half-planes cross(e_i, p - s_i) >= 0
-    {
-        float t0 = 0.f, t1 = 1.f;
-        bool keep = true;
+    float t0 = 0.f, t1 = 1.f;
+    bool keep = true;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const float2 e = sub2(F.s[(i + 1) & 3], F.s[i]);
-            // cross(e, (X1, t Y1) - s_i) = cross(e, (X1, 0) - s_i) + t Y1 e.x
-            const float p = e.x * (0.f - F.s[i].y) - e.y * (X1 - F.s[i].x), q = e.x * Y1;
-            const bool k = clip_t(p, q, q != 0.f ? 1.f / q : 0.f, t0, t1);
-            // a quad edge on the line x = X1: the box edge is kept if the quad lies beyond it, or on it running
-            // downward (the two cancel); running upward the quad edge itself is the boundary, counted once
-            keep = keep & (q == 0.f ? (p > 0.f || (p == 0.f && e.y < 0.f)) : k);
-        }
-        sk[4] = keep && t0 < t1;
-        sa[4] = make_float2(X1, t0 * Y1);
-        sb[4] = make_float2(X1, t1 * Y1);
+    for (int i = 0; i < 4; ++i) {
+        const float2 e = sub2(F.s[(i + 1) & 3], F.s[i]);
+        // cross(e, (X1, t Y1) - s_i) = cross(e, (X1, 0) - s_i) + t Y1 e.x
+        const float p = e.x * (0.f - F.s[i].y) - e.y * (X1 - F.s[i].x), q = e.x * Y1;
+        const bool k = clip_t(p, q, q != 0.f ? 1.f / q : 0.f, t0, t1);
+        // a quad edge on the line x = X1: the box edge is kept if the quad lies beyond it, or on it running
+        // downward (the two cancel); running upward the quad edge itself is the boundary, counted once
+        keep = keep & (q == 0.f ? (p > 0.f || (p == 0.f && e.y < 0.f)) : k);
     }
-#pragma unroll 1
-    for (int i = 0; i < 5; ++i) {
-        if (sk[0]) walk_cells(sa[0], sb[0], rx, ry, visit);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {  // next segment into slot 0 (static indices: the arrays stay in registers)
-            sa[j] = sa[j + 1];
-            sb[j] = sb[j + 1];
-            sk[j] = sk[j + 1];
-        }
-    }
+    sk[4] = keep && t0 < t1;
+    sa[4] = make_float2(X1, t0 * Y1);
+    sb[4] = make_float2(X1, t1 * Y1);
 }
 
-// The footprint integral (before the division by the area) of a convex footprint, from the texture and its
-// row-prefix table P (the splat's [ry, rx] float4 rows).  (Gathering the weights per cell to read each texel
-// once, as the adjoint's scatter does for its atomics, measured 1.6x slower here: the loads hit L1.)
+// The integral of F dy along one boundary segment a -> b, F measured from column x0 (see above), from the
+// splat's texture and its row-prefix table P ([ry, rx] float4 rows).  (Keeping the texels of the cell being
+// walked in registers, to read only the two a step to the next cell does not share, measured 1.8x slower:
+// the loads hit L1, the branches do not pay.)
 template <class Tex>
-__device__ __forceinline__ float4 aniso_boundary_sum_impl(const FootQuad& F, const void* textures, int64_t tex_base,
-                                                          const float4* P, int rx, int ry, float scale) {
+__device__ __forceinline__ float4 segment_sum(float2 a, float2 b, int x0, const void* textures, int64_t tex_base,
+                                              const float4* P, int rx, int ry, float scale) {
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (!(F.maxu > F.minu && F.maxv > F.minv)) return acc;  // no cell (also: rx or ry below 2)
-    const int x0 = F.minu;
-    foot_boundary(F, rx, ry, [&](float2 a, float2 b, int u, int v) {
-        const PieceW w = piece_weights(a, b, u, v);
+    walk_cells(a, b, rx, ry, [&](float2 pa, float2 pb, int u, int v) {
+        const PieceW w = piece_weights(pa, pb, u, v);
         const int64_t t00 = tex_base + (int64_t)v * rx + u;
         const float4 ta = Tex::load(textures, t00, scale), tb = Tex::load(textures, t00 + 1, scale);
         const float4 tc = Tex::load(textures, t00 + rx, scale), td = Tex::load(textures, t00 + rx + 1, scale);
@@ -414,25 +402,24 @@ __device__ __forceinline__ float4 aniso_boundary_sum_impl(const FootQuad& F, con
     return acc;
 }
 
-// The same sum as one out-of-line copy, for the adjoint (which also has the scatter's walk: both inlined
+// The same as one out-of-line copy, for the adjoint (which also has the scatter's walk: both inlined
 // outgrow the instruction cache).
 template <class Tex>
-static __device__ __noinline__ float4 aniso_boundary_sum_shared(const FootQuad F, const void* textures,
-                                                                int64_t tex_base, const float4* P, int rx, int ry,
-                                                                float scale) {
-    return aniso_boundary_sum_impl<Tex>(F, textures, tex_base, P, rx, ry, scale);
+static __device__ __noinline__ float4 segment_sum_shared(float2 a, float2 b, int x0, const void* textures,
+                                                         int64_t tex_base, const float4* P, int rx, int ry,
+                                                         float scale) {
+    return segment_sum<Tex>(a, b, x0, textures, tex_base, P, rx, ry, scale);
 }
 
-// Adjoint of aniso_boundary_sum for the gradient g (already divided by the area): texel gradients into vt
-// (the splat's [ry, rx] float4 rows) and row-prefix gradients into vP, which tg_rasterize_bwd folds back
-// into the texels afterwards.  The x0 terms of the sum are left out here: they integrate a function of y
-// alone around the closed boundary, which is zero, so the gradient is the same without them (and the
-// column x0 would take an atomic from every piece).  Weights of the cell being walked are kept in registers
-// and flushed when the walk leaves it; the two texels (and one prefix entry) a cell shares with the next
-// one along the walk carry over, so a piece costs about two texel atomics and one prefix atomic.
-static __device__ __noinline__ void aniso_boundary_scatter(const FootQuad F, float4 g, float* vt, float* vP, int rx,
-                                                           int ry) {
-    if (!(F.maxu > F.minu && F.maxv > F.minv)) return;
+// Adjoint of segment_sum for the gradient g (already divided by the area): texel gradients into vt (the
+// splat's [ry, rx] float4 rows) and row-prefix gradients into vP, which tg_rasterize_bwd folds back into the
+// texels afterwards.  The x0 terms are left out: over the closed boundary they integrate a function of y
+// alone, which gives zero, so the footprint's gradient is the same without them (and the column x0 would
+// take an atomic from every piece).  The weights of the cell being walked stay in registers until the walk
+// leaves it; the two texels (and the prefix entry) a cell shares with the next one carry over, so a piece
+// costs about two texel atomics and one prefix atomic.
+static __device__ __noinline__ void segment_scatter(float2 a, float2 b, float4 g, float* vt, float* vP, int rx,
+                                                    int ry) {
     float4* T4 = reinterpret_cast<float4*>(vt);
     float4* P4 = reinterpret_cast<float4*>(vP);
     auto put = [&](float4* base, int64_t i, float w) {
@@ -449,7 +436,7 @@ static __device__ __noinline__ void aniso_boundary_scatter(const FootQuad F, flo
     };
     int cu = -1, cv = -1;
     float wa = 0.f, wb = 0.f, wc = 0.f, wd = 0.f, w0 = 0.f, w1 = 0.f;  // the current cell's pending weights
-    foot_boundary(F, rx, ry, [&](float2 a, float2 b, int u, int v) {
+    walk_cells(a, b, rx, ry, [&](float2 pa, float2 pb, int u, int v) {
         if (u != cu || v != cv) {
             float na = 0.f, nb = 0.f, nc = 0.f, nd = 0.f, n0 = 0.f, n1 = 0.f;
             if (cu >= 0) {
@@ -464,24 +451,104 @@ static __device__ __noinline__ void aniso_boundary_scatter(const FootQuad F, flo
             cv = v;
             wa = na; wb = nb; wc = nc; wd = nd; w0 = n0; w1 = n1;
         }
-        const PieceW w = piece_weights(a, b, u, v);
+        const PieceW w = piece_weights(pa, pb, u, v);
         wa += w.wa; wb += w.wb; wc += w.wc; wd += w.wd; w0 += w.wp0; w1 += w.wp1;
     });
     if (cu >= 0) flush(cu, cv, wa, wb, wc, wd, w0, w1);
 }
 
-__device__ __forceinline__ FootQuad foot_quad(const AnisoFoot& F) {
-    FootQuad Q;
+// Per-warp shared memory of the boundary integration: the warp's clipped segments (up to five for each of
+// its 32 footprints), each segment's owner lane (and x0), and one float4 per lane.
+constexpr int kAnisoSegs = 5 * 32;
+constexpr int kAnisoWarpF4 = kAnisoSegs + 32 + kAnisoSegs / 4;  // segments, per-lane slots, owners (int)
+struct AnisoWarp {
+    float4* seg;  // [kAnisoSegs] (a.x, a.y, b.x, b.y)
+    float4* lane; // [32]
+    int* own;     // [kAnisoSegs] owner lane | x0 << 5
+};
+__device__ __forceinline__ AnisoWarp aniso_warp(float4* base) {
+    return AnisoWarp{base, base + kAnisoSegs, reinterpret_cast<int*>(base + kAnisoSegs + 32)};
+}
+
+// Lists the kept boundary segments of every lane with want set (a convex footprint with cells to
+// integrate) in the warp's shared memory, in lane order; returns how many there are.  The segments are then
+// spread over the warp's lanes: a warp typically has a handful of footprints of four segments each, so
+// integrating each footprint on its own lane leaves most lanes idle behind the longest boundary.  (Cutting
+// the segments further into chunks of a few cells, to fill all 32 lanes, measured slower: 5-27 %.)
+__device__ __forceinline__ int aniso_gather(const AnisoFoot& F, bool want, int rx, int ry, const AnisoWarp& W,
+                                            unsigned mask) {
+    const int lane = threadIdx.x & 31;
+    float2 sa[5], sb[5];
+    bool sk[5] = {false, false, false, false, false};
+    if (want) foot_segments(F, rx, ry, sa, sb, sk);
+    int n = 0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        Q.s[i] = F.s[i];
-        Q.r[i] = F.r[i];
+    for (int i = 0; i < 5; ++i) {
+        sk[i] = sk[i] && want;
+        n += sk[i];
     }
-    Q.minu = F.minu;
-    Q.maxu = F.maxu;
-    Q.minv = F.minv;
-    Q.maxv = F.maxv;
-    return Q;
+    int incl = n;  // inclusive warp scan of the counts
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(mask, incl, o);
+        if (lane >= o) incl += t;
+    }
+    int j = incl - n;
+    const int tag = lane | (F.minu << 5);
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+        if (sk[i]) {
+            W.seg[j] = make_float4(sa[i].x, sa[i].y, sb[i].x, sb[i].y);
+            W.own[j] = tag;
+            ++j;
+        }
+    return __shfl_sync(mask, incl, 31);
+}
+
+// Every lane's footprint integral (before the division by the area) for the lanes with want set, the warp's
+// boundary segments spread over its lanes and summed per owner in shared memory.  Called by the full warp.
+template <class Tex, bool kShared>
+__device__ __forceinline__ float4 aniso_boundary_sum(const AnisoFoot& F, bool want, const void* textures,
+                                                     int64_t tex_base, const float4* P, int rx, int ry, float scale,
+                                                     const AnisoWarp& W, unsigned mask) {
+    const int lane = threadIdx.x & 31;
+    want = want && F.maxu > F.minu && F.maxv > F.minv;  // no cell (also: rx or ry below 2): nothing to walk
+    const int n = aniso_gather(F, want, rx, ry, W, mask);
+    W.lane[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncwarp(mask);
+    for (int t = lane; t < n; t += 32) {
+        const float4 sg = W.seg[t];
+        const int ow = W.own[t];
+        const float2 a = make_float2(sg.x, sg.y), b = make_float2(sg.z, sg.w);
+        float4 r;
+        if constexpr (kShared) r = segment_sum_shared<Tex>(a, b, ow >> 5, textures, tex_base, P, rx, ry, scale);
+        else r = segment_sum<Tex>(a, b, ow >> 5, textures, tex_base, P, rx, ry, scale);
+        float* dst = reinterpret_cast<float*>(W.lane + (ow & 31));
+        atomicAdd(dst, r.x);
+        atomicAdd(dst + 1, r.y);
+        atomicAdd(dst + 2, r.z);
+        atomicAdd(dst + 3, r.w);
+    }
+    __syncwarp(mask);
+    const float4 r = W.lane[lane];
+    __syncwarp(mask);  // read before the next call reuses the slots
+    return r;
+}
+
+// Adjoint of aniso_boundary_sum: the gradient g of every lane with want set (already divided by the area)
+// scattered along its footprint's boundary, the segments spread over the warp.  Called by the full warp.
+__device__ __forceinline__ void aniso_boundary_scatter(const AnisoFoot& F, float4 g, bool want, float* vt, float* vP,
+                                                       int rx, int ry, const AnisoWarp& W, unsigned mask) {
+    const int lane = threadIdx.x & 31;
+    want = want && F.maxu > F.minu && F.maxv > F.minv;
+    const int n = aniso_gather(F, want, rx, ry, W, mask);
+    W.lane[lane] = g;
+    __syncwarp(mask);
+    for (int t = lane; t < n; t += 32) {
+        const float4 sg = W.seg[t];
+        segment_scatter(make_float2(sg.x, sg.y), make_float2(sg.z, sg.w), W.lane[W.own[t] & 31], vt, vP, rx, ry);
+    }
+    __syncwarp(mask);  // done with the slots before the next call reuses them
 }
 
 // Bilinear weights of a cell's four texels (u,v), (u+1,v), (u,v+1), (u+1,v+1) from its moments.
@@ -748,17 +815,15 @@ __device__ __forceinline__ void foot_cell(const AnisoFoot& F, int i, int& u, int
 template <class Tex, bool kShared = false>
 __device__ __forceinline__ float4 aniso_coop_sum(const AnisoFoot& Fown, bool need, const void* textures,
                                                  int64_t tex_base, int rx, float scale, unsigned mask,
-                                                 const float4* P = nullptr, int ry = 0) {
+                                                 const float4* P = nullptr, int ry = 0, float4* s_warp = nullptr) {
     const int lane = threadIdx.x & 31;
     float4 mine = make_float4(0.f, 0.f, 0.f, 0.f);
-    // with the row-prefix table, each lane integrates its own convex footprint along its boundary; the warp
-    // integrates the others together, cell by cell
-    if (P != nullptr && need && Fown.convex) {
-        if constexpr (kShared)
-            mine = aniso_boundary_sum_shared<Tex>(foot_quad(Fown), textures, tex_base, P, rx, ry, scale);
-        else
-            mine = aniso_boundary_sum_impl<Tex>(foot_quad(Fown), textures, tex_base, P, rx, ry, scale);
-        need = false;
+    // with the row-prefix table, convex footprints are integrated along their boundaries (P is the same for
+    // the whole warp); the others cell by cell
+    if (P != nullptr) {
+        mine = aniso_boundary_sum<Tex, kShared>(Fown, need && Fown.convex, textures, tex_base, P, rx, ry, scale,
+                                                aniso_warp(s_warp), mask);
+        need = need && !Fown.convex;
     }
     unsigned pending = __ballot_sync(mask, need);
     while (pending) {
@@ -792,11 +857,12 @@ __device__ __forceinline__ float4 aniso_coop_sum(const AnisoFoot& Fown, bool nee
 // already divided by the area; need: it has one), cells spread over the warp.
 template <bool kShared = false>
 __device__ __forceinline__ void aniso_coop_scatter(const AnisoFoot& Fown, float4 gown, bool need, float* vt, int rx,
-                                                   unsigned mask, float* vP = nullptr, int ry = 0) {
+                                                   unsigned mask, float* vP = nullptr, int ry = 0,
+                                                   float4* s_warp = nullptr) {
     const int lane = threadIdx.x & 31;
-    if (vP != nullptr && need && Fown.convex) {
-        aniso_boundary_scatter(foot_quad(Fown), gown, vt, vP, rx, ry);
-        need = false;
+    if (vP != nullptr) {  // uniform over the warp
+        aniso_boundary_scatter(Fown, gown, need && Fown.convex, vt, vP, rx, ry, aniso_warp(s_warp), mask);
+        need = need && !Fown.convex;
     }
     unsigned pending = __ballot_sync(mask, need);
     while (pending) {
@@ -830,14 +896,15 @@ __device__ __forceinline__ void eval_aniso_coop(PairEvalAniso& e, bool act, floa
                                                 const float4 m0, const float4 m1, const float4 m2,
                                                 const void* textures, int64_t tex_base, int rx, int ry, float range_x,
                                                 float range_y, float g_weight, unsigned mask,
-                                                const float4* P = nullptr) {
+                                                const float4* P = nullptr, float4* s_warp = nullptr) {
     e.valid = false;
     e.need = false;
     e.tex_valid = false;
     if (act)
         eval_pair<Tex, FiltAniso>(e, px, py, xyo, m0, m1, m2, textures, tex_base, rx, ry, range_x, range_y, g_weight);
     const bool need = act && e.valid && e.need;
-    const float4 ts = aniso_coop_sum<Tex, kShared>(e.F, need, textures, tex_base, rx, xyo.w, mask, P, ry);
+    if (need && (P == nullptr || !e.F.convex)) aniso_cells_setup(e.F);  // integrated cell by cell
+    const float4 ts = aniso_coop_sum<Tex, kShared>(e.F, need, textures, tex_base, rx, xyo.w, mask, P, ry, s_warp);
     if (!(act && e.valid)) return;
     e.asf = 0.f;
     if (need) {

@@ -54,6 +54,9 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
     float4* s_nrm = s_m2 + bs;
     float* s_col = reinterpret_cast<float*>(s_nrm + bs);
     int* s_row = reinterpret_cast<int*>(s_col + bs * D);
+    // anisotropic_bilinear: the boundary integration's per-warp area (16-byte aligned: bs is a multiple of 32)
+    float4* s_aniso = Filt::kAniso ? reinterpret_cast<float4*>(s_row + bs) + (threadIdx.x >> 5) * kAnisoWarpF4
+                                   : nullptr;
 
     const unsigned wmask = __activemask();
     const TileWork tc = tile_work(a, item);
@@ -173,7 +176,8 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
                     eval_aniso_coop<Tex>(e, act, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx,
                                          a.tex_ry, a.range_x, a.range_y, a.g_weight, wmask,
                                          a.aniso_prefix ? reinterpret_cast<const float4*>(a.aniso_prefix) + tex_base
-                                                        : nullptr);
+                                                        : nullptr,
+                                         s_aniso);
                     if (!act) continue;
                 } else {
                     if (!act) continue;
@@ -274,7 +278,7 @@ template <int D, class Tex, class Filt>
 cudaError_t launch_fwd_filter(const tg_raster_fwd_args& a, cudaStream_t s) {
     const int tile_px = a.tile_size * a.tile_size;
     const int bs = a.batch_depth > 0 ? a.batch_depth : tile_px;
-    const size_t smem = fwd_smem_bytes(D, bs);
+    const size_t smem = fwd_smem_bytes(D, bs) + (Filt::kAniso ? (size_t)(tile_px / 32) * kAnisoWarpF4 * 16 : 0);
     const int64_t blocks = a.views ? a.n_tiles : (int64_t)a.C * a.tile_width * a.tile_height;
     if (blocks == 0) return cudaSuccess;
     cudaError_t err = cudaFuncSetAttribute(raster_fwd_kernel<D, Tex, 1, false, Filt>,
