@@ -426,6 +426,17 @@ typedef struct {
      * instead of cell by cell as the reference does; the same integral up to
      * FP32 rounding.  No counterpart in the reference. */
     const float* aniso_prefix;
+    /* With aniso_prefix: records of the footprint integrals the forward
+     * computes, per pixel in the order it computes them: aniso_records
+     * [n_pixels, aniso_record_cap, 4] FP32 (the first aniso_record_cap of
+     * each pixel's) and aniso_record_count [n_pixels] int32 (how many of them
+     * the pixel had up to its last contributor).  Given the same pointers the
+     * adjoint reads these integrals instead of integrating the footprints
+     * again (those past the capacity it integrates again).  NULL / 0: none.
+     * No counterpart in the reference. */
+    float* aniso_records;
+    int32_t* aniso_record_count;
+    int32_t aniso_record_cap;
 } tg_raster_fwd_args;
 TG_API int tg_rasterize_fwd(const tg_raster_fwd_args* a, tg_stream_t stream);
 

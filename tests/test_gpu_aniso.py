@@ -208,3 +208,31 @@ def test_aniso_boundary_and_cells_agree_on_a_large_scene(integration):
     for i, name in enumerate(("colors", "alphas")):
         assert_close(outs["boundary"][i], outs["cells"][i], 1e-5, 1e-5, 1e-3, name)
     assert rel_l2(outs["boundary"][2], outs["cells"][2]) < 1e-4
+
+
+@pytest.mark.parametrize("name", ["small", "adjoint"])
+def test_aniso_adjoint_from_forward_records_matches_integrating_again(name, integration, monkeypatch):
+    """The adjoint reading the forward's footprint integrals (all of them, or only each pixel's first two: the
+    rest integrated again) against the adjoint integrating every footprint again."""
+    if integration != "boundary":
+        pytest.skip("records exist with the boundary integration only")
+    s = SCENES[name]()
+    d = _inputs(s, 8)
+    C, H, Wd = d["C"], s.height, s.width
+    rng = np.random.default_rng(5)
+    up_c = T(rng.normal(size=(C, H, Wd, 3)).astype(np.float32))
+    up_a = T(rng.normal(size=(C, H, Wd, 1)).astype(np.float32))
+    grads = {}
+    for cap in (0, 2, 32):
+        monkeypatch.setattr(W, "ANISO_RECORDS", cap)
+        leaves = [d["means2d"].detach().clone().requires_grad_(), d["M"].detach().clone().requires_grad_(),
+                  T(d["colors"]).requires_grad_(), T(d["opac"]).requires_grad_(), d["tex"].detach().clone().requires_grad_()]
+        out = rasterize_to_pixels_textured_gaussians(
+            leaves[0], leaves[1], leaves[2], leaves[3], leaves[4], 3.0, 3.0, d["normals"],
+            torch.zeros_like(d["means2d"]), Wd, H, 8, d["off"], d["fl"], filtering="anisotropic_bilinear")
+        ((out[0] * up_c).sum() + (out[1] * up_a).sum()).backward()
+        grads[cap] = [to_np(x.grad) for x in leaves]
+    for cap in (2, 32):
+        for k, (got, ref) in enumerate(zip(grads[cap], grads[0])):
+            assert np.abs(ref).max() > 0
+            assert rel_l2(got, ref) < 1e-6, (cap, k, rel_l2(got, ref))

@@ -81,7 +81,8 @@ class RasterFwdArgs(ctypes.Structure):
                 ("last_ids", P), ("median_ids", P), ("contrib_sum", P), ("contrib_count", P), ("tile_order", P),
                 ("views", P), ("tile_view", P), ("n_tiles", I64), ("n_pixels", I64), ("n_isects_dev", P),
                 ("batch_depth", I32), ("work_queue", P), ("mip_levels", I32), ("tex_coarse", P),
-                ("filter", I32), ("t_checkpoints", P), ("aniso_prefix", P)]
+                ("filter", I32), ("t_checkpoints", P), ("aniso_prefix", P),
+                ("aniso_records", P), ("aniso_record_count", P), ("aniso_record_cap", I32)]
 
 
 class RasterBwdArgs(ctypes.Structure):

@@ -174,6 +174,9 @@ int check_raster_common(const tg_raster_fwd_args& a) {
                    "the anisotropic_bilinear filter runs with tile 8 or 16 and one CTA per tile");
         TG_REQUIRE(a.aniso_prefix == nullptr || aligned(a.aniso_prefix, 16), TG_ERR_INVALID_ARG,
                    "aniso_prefix must be 16-byte aligned");
+        TG_REQUIRE(a.aniso_records == nullptr ||
+                       (a.aniso_record_count != nullptr && a.aniso_record_cap > 0 && aligned(a.aniso_records, 16)),
+                   TG_ERR_INVALID_ARG, "aniso_records needs a 16-byte aligned buffer, counts and a capacity");
     }
     return TG_OK;
 }

@@ -85,6 +85,7 @@ struct PixelAdj {
     float acc_d_buf, acc_d, acc_w_buf, acc_w, dist_buf;
     int32_t local;     // pixel index within the tile
     int32_t ck_batch;  // forward batch whose end transmittance T was last restarted from (-1: none)
+    int32_t rec;       // anisotropic_bilinear: the forward's record of the next footprint integral (counting down)
 };
 
 // The forward's transmittance checkpoints of one tile (tg_raster_fwd_args.t_checkpoints): base is the tile's
@@ -306,6 +307,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
         p.inside = p.pix >= 0;
         p.local = local;
         p.ck_batch = -1;
+        p.rec = -1;
         p.px = (float)j + 0.5f;
         p.py = (float)i + 0.5f;
         p.T_final = 1.f; p.v_a = p.v_dist = p.v_med = p.bg_dot = 0.f;
@@ -321,6 +323,7 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
             p.T_final = 1.f - alpha_out;
             p.bin_final = a.last_ids[px_];
             p.median_idx = a.median_ids[px_];
+            if (Filt::kAniso && f.aniso_records != nullptr) p.rec = f.aniso_record_count[px_] - 1;
 #pragma unroll
             for (int k = 0; k < D; ++k) p.v_c[k] = a.v_render_colors[px_ * D + k];
             p.v_a = a.v_render_alphas[px_];
@@ -401,12 +404,19 @@ __device__ __forceinline__ void bwd_tile(const tg_raster_bwd_args& a, const floa
             for (int q = 0; q < PPT; ++q) {
                 if constexpr (Filt::kAniso) {  // every lane takes part: the warp integrates footprints together
                     const bool act = P[q].inside && idx <= P[q].bin_final && in_box(box, P[q].px, P[q].py);
+                    // the forward's integral of this pair's footprint, if it has one (it keeps the first
+                    // aniso_record_cap of each pixel's, in order; this walks them back to front)
+                    const float4* rec = act && P[q].rec >= 0 && P[q].rec < f.aniso_record_cap
+                                            ? reinterpret_cast<const float4*>(f.aniso_records) +
+                                                  P[q].pix * f.aniso_record_cap + P[q].rec
+                                            : nullptr;
                     PairOf<Filt> e;
                     eval_aniso_coop<Tex, true>(e, act, P[q].px, P[q].py, xyo, m0, m1, m2, f.textures, tex_base, f.tex_rx,
                                          f.tex_ry, f.range_x, f.range_y, f.g_weight, wmask,
                                          f.aniso_prefix ? reinterpret_cast<const float4*>(f.aniso_prefix) + tex_base
                                                         : nullptr,
-                                         s_aniso);
+                                         s_aniso, rec);
+                    if (e.tex_valid) --P[q].rec;  // this pair's footprint was integrated (or read): one record
                     const bool use = act && e.valid;
                     float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (use) {

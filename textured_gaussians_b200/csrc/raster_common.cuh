@@ -896,15 +896,18 @@ __device__ __forceinline__ void eval_aniso_coop(PairEvalAniso& e, bool act, floa
                                                 const float4 m0, const float4 m1, const float4 m2,
                                                 const void* textures, int64_t tex_base, int rx, int ry, float range_x,
                                                 float range_y, float g_weight, unsigned mask,
-                                                const float4* P = nullptr, float4* s_warp = nullptr) {
+                                                const float4* P = nullptr, float4* s_warp = nullptr,
+                                                const float4* rec = nullptr) {
     e.valid = false;
     e.need = false;
     e.tex_valid = false;
     if (act)
         eval_pair<Tex, FiltAniso>(e, px, py, xyo, m0, m1, m2, textures, tex_base, rx, ry, range_x, range_y, g_weight);
     const bool need = act && e.valid && e.need;
-    if (need && (P == nullptr || !e.F.convex)) aniso_cells_setup(e.F);  // integrated cell by cell
-    const float4 ts = aniso_coop_sum<Tex, kShared>(e.F, need, textures, tex_base, rx, xyo.w, mask, P, ry, s_warp);
+    const bool have = need && rec != nullptr;  // rec: the forward's record of this footprint's integral
+    if (need && (P == nullptr || !e.F.convex)) aniso_cells_setup(e.F);  // integrated (or scattered) cell by cell
+    float4 ts = aniso_coop_sum<Tex, kShared>(e.F, need && !have, textures, tex_base, rx, xyo.w, mask, P, ry, s_warp);
+    if (have) ts = *rec;
     if (!(act && e.valid)) return;
     e.asf = 0.f;
     if (need) {

@@ -117,6 +117,9 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
 
     float T[PPT], pix_out[PPT][D], nrm_out[PPT][3], distort[PPT], accum_vis_depth[PPT], median_depth[PPT];
     int32_t cur_idx[PPT], median_idx[PPT];
+    // anisotropic_bilinear records: footprint integrals computed so far, and those up to the last contributor
+    int32_t rec_n[PPT], rec_last[PPT];
+    const bool records = Filt::kAniso && a.aniso_records != nullptr;
 #pragma unroll
     for (int q = 0; q < PPT; ++q) {
         T[q] = 1.f;
@@ -125,6 +128,7 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
         nrm_out[q][0] = nrm_out[q][1] = nrm_out[q][2] = 0.f;
         distort[q] = accum_vis_depth[q] = median_depth[q] = 0.f;
         cur_idx[q] = median_idx[q] = 0;
+        rec_n[q] = rec_last[q] = 0;
     }
 
     for (int b = 0; b < num_batches; ++b) {
@@ -179,6 +183,12 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
                                                         : nullptr,
                                          s_aniso);
                     if (!act) continue;
+                    if (records && e.tex_valid) {  // every integral, in order, whether or not the pair is kept
+                        if (rec_n[q] < a.aniso_record_cap)
+                            reinterpret_cast<float4*>(a.aniso_records)[pix[q] * a.aniso_record_cap + rec_n[q]] =
+                                e.tsum;
+                        ++rec_n[q];
+                    }
                 } else {
                     if (!act) continue;
                     eval_pair<Tex, Filt>(e, px[q], py[q], xyo, m0, m1, m2, a.textures, tex_base, a.tex_rx, a.tex_ry,
@@ -207,6 +217,7 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
                     median_idx[q] = batch_start + t;
                 }
                 cur_idx[q] = batch_start + t;
+                rec_last[q] = rec_n[q];
                 T[q] = next_T;
                 if (e.alpha > a.contrib_threshold) {
                     csum += e.alpha;
@@ -245,6 +256,7 @@ __device__ __forceinline__ void fwd_tile(const tg_raster_fwd_args& a, const int 
         a.out_distort[p] = distort[q];
         a.out_median[p] = median_depth[q];
         a.median_ids[p] = median_idx[q];
+        if (records) a.aniso_record_count[p] = rec_last[q];
     }
 }
 

@@ -618,6 +618,9 @@ def generate_mipmap(textures: Tensor, log_texture_res: int, log_reduce: int = 4,
 # boundary, over row-prefix tables built per call by tg_aniso_prefix; the others cell by cell) or "cells"
 # (every footprint cell by cell, as the reference does).  The same integral up to FP32 rounding.
 ANISO_INTEGRATION = "boundary"
+# Footprint integrals per pixel the forward keeps for the adjoint with the boundary integration (0: none;
+# the adjoint then integrates every footprint again).  Each pixel's first ANISO_RECORDS are kept.
+ANISO_RECORDS = 32
 
 
 def _aniso_prefix(tex_store, tex_scales, st):
@@ -713,6 +716,13 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         st = B.stream_of(means2d)
         prefix = _aniso_prefix(tex_store, tex_scales, st) if filter_code == B.TG_FILTER_ANISO_BILINEAR else None
         a.aniso_prefix = B.ptr(prefix)
+        # the footprint integrals, kept for the adjoint (which then need not integrate them again)
+        records = counts = None
+        if prefix is not None and ANISO_RECORDS > 0 and any(ctx.needs_input_grad):
+            n_pix = math.prod(pshape)
+            records = torch.empty((n_pix, ANISO_RECORDS, 4), dtype=torch.float32, device=dev)
+            counts = torch.empty((n_pix,), dtype=torch.int32, device=dev)
+            a.aniso_records, a.aniso_record_count, a.aniso_record_cap = B.ptr(records), B.ptr(counts), ANISO_RECORDS
         B.call("tg_rasterize_fwd", st, B.lib().tg_rasterize_fwd, ctypes.byref(a), st)
         ctx.save_for_backward(means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, m,
                               tex_store, tex_scales, isect_offsets, flatten_ids, render_colors, render_alphas,
@@ -724,6 +734,7 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         ctx.mip = (mip_levels, coarse, filter_code)
         ctx.t_checkpoints = ckpt
         ctx.aniso_prefix = prefix
+        ctx.aniso_records = (records, counts)
         ctx.mark_non_differentiable(contrib_sum, contrib_count)
         return render_colors, render_alphas, render_normals, render_distort, render_median, contrib_sum, contrib_count
 
@@ -751,6 +762,9 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
                       0.0, g_weight, C, N, ctx.layout, ctx.n_isects_dev, *ctx.mip)
         f.t_checkpoints = B.ptr(ctx.t_checkpoints)
         f.aniso_prefix = B.ptr(ctx.aniso_prefix)
+        if ctx.aniso_records[0] is not None:
+            f.aniso_records, f.aniso_record_count = B.ptr(ctx.aniso_records[0]), B.ptr(ctx.aniso_records[1])
+            f.aniso_record_cap = ctx.aniso_records[0].shape[1]
         v_means2d = torch.empty_like(means2d)
         v_means2d_abs = torch.empty_like(means2d) if absgrad else None
         v_ray_transforms = torch.empty_like(ray_transforms)
