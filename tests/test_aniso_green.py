@@ -13,9 +13,8 @@ footprint's first cell column) to x, read from the rows' prefix integrals:
 the quad's edges clipped to the grid plus the grid's right edge inside the
 quad, walked cell by cell, each piece integrated by two-point Gauss-Legendre
 (exact: F is cubic along a piece).  The adjoint leaves out the x0 terms (they
-integrate a function of y alone around a closed curve), carries the weights of
-texels shared by consecutive cells, and accumulates prefix-table gradients
-that a transposed scan folds back into the texels.
+integrate a function of y alone around a closed curve) and accumulates
+prefix-table gradients that a transposed scan folds back into the texels.
 
 This test restates those steps in FP64 and checks (1) the filtered value
 against the oracle on quads built to hit the special cases -- edges on grid
@@ -149,42 +148,22 @@ def boundary_integral(corners, tex):
 
 
 def boundary_adjoint(corners, g, shape):
-    """segment_scatter (no x0 terms, shared texels carried between consecutive cells) plus the prefix fold."""
+    """segment_scatter (each piece's six weights, no x0 terms) plus the prefix fold."""
     ry, rx = shape[:2]
     s, _ = _oriented(corners)
     minu, maxu, minv, maxv = _cell_range(s, rx, ry)
     vt, vP = np.zeros(shape), np.zeros(shape)
     if not (maxu > minu and maxv > minv):
         return vt
-
-    def flush(u, v, w):
-        vt[v, u] += g * w[0]
-        vt[v, u + 1] += g * w[1]
-        vt[v + 1, u] += g * w[2]
-        vt[v + 1, u + 1] += g * w[3]
-        vP[v, u] += g * w[4]
-        vP[v + 1, u] += g * w[5]
-
     for a, b in _segments(s, rx, ry):
-        cu = cv = -1
-        w = np.zeros(6)
         for pa, pb, u, v in _walk(a, b, rx, ry):
-            if (u, v) != (cu, cv):
-                n = np.zeros(6)
-                if cu >= 0:
-                    if v == cv and u == cu + 1:
-                        n[0], n[2], w[1], w[3] = w[1], w[3], 0, 0
-                    elif v == cv and u == cu - 1:
-                        n[1], n[3], w[0], w[2] = w[0], w[2], 0, 0
-                    elif u == cu and v == cv + 1:
-                        n[0], n[1], n[4], w[2], w[3], w[5] = w[2], w[3], w[5], 0, 0, 0
-                    elif u == cu and v == cv - 1:
-                        n[2], n[3], n[5], w[0], w[1], w[4] = w[0], w[1], w[4], 0, 0, 0
-                    flush(cu, cv, w)
-                cu, cv, w = u, v, n
-            w = w + _weights(pa, pb, u, v)
-        if cu >= 0:
-            flush(cu, cv, w)
+            w = _weights(pa, pb, u, v)
+            vt[v, u] += g * w[0]
+            vt[v, u + 1] += g * w[1]
+            vt[v + 1, u] += g * w[2]
+            vt[v + 1, u + 1] += g * w[3]
+            vP[v, u] += g * w[4]
+            vP[v + 1, u] += g * w[5]
     # the fold (aniso_prefix_fold_kernel): dt(0) = S(1) / 2, dt(j) = (S(j) + S(j+1)) / 2, S(j) = sum_{u>=j} dP[u]
     for r in range(ry):
         dP = vP[r].copy()
