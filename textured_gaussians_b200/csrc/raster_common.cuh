@@ -432,9 +432,11 @@ static __device__ __noinline__ void segment_scatter(float2 a, float2 b, float4 g
     });
 }
 
-// Per-warp shared memory of the boundary integration: the warp's clipped segments (up to five for each of
-// its 32 footprints), each segment's owner lane (and x0), and one float4 per lane.
-constexpr int kAnisoSegs = 5 * 32;
+// Per-warp shared memory of the boundary integration: a list of the warp's clipped boundary segments (up to
+// kAnisoSegs at a time: a warp pass has 19 on average, at most 5 for each of its 32 footprints), each
+// segment's owner lane (and x0), and one float4 per lane.  Small on purpose: the compositor's shared memory
+// comes out of the L1 that the boundary walk reads the texture through.
+constexpr int kAnisoSegs = 64;
 constexpr int kAnisoWarpF4 = kAnisoSegs + 32 + kAnisoSegs / 4;  // segments, per-lane slots, owners (int)
 struct AnisoWarp {
     float4* seg;  // [kAnisoSegs] (a.x, a.y, b.x, b.y)
@@ -445,22 +447,24 @@ __device__ __forceinline__ AnisoWarp aniso_warp(float4* base) {
     return AnisoWarp{base, base + kAnisoSegs, reinterpret_cast<int*>(base + kAnisoSegs + 32)};
 }
 
-// Lists the kept boundary segments of every lane with want set (a convex footprint with cells to
-// integrate) in the warp's shared memory, in lane order; returns how many there are.  The segments are then
-// spread over the warp's lanes: a warp typically has a handful of footprints of four segments each, so
-// integrating each footprint on its own lane leaves most lanes idle behind the longest boundary.  (Cutting
-// the segments further into chunks of a few cells, to fill all 32 lanes, measured slower: 5-27 %.)
-__device__ __forceinline__ int aniso_gather(const AnisoFoot& F, bool want, int rx, int ry, const AnisoWarp& W,
-                                            unsigned mask) {
-    const int lane = threadIdx.x & 31;
+// The kept boundary segments of a lane's footprint (want: a convex footprint with cells to integrate) and
+// their position in the warp's list (lane order): the segments base .. base + n - 1 of total.
+struct SegList {
     float2 sa[5], sb[5];
-    bool sk[5] = {false, false, false, false, false};
-    if (want) foot_segments(F, rx, ry, sa, sb, sk);
+    bool sk[5];
+    int base, total;
+};
+__device__ __forceinline__ void aniso_segments(const AnisoFoot& F, bool want, int rx, int ry, unsigned mask,
+                                               SegList& L) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) L.sk[i] = false;
+    if (want) foot_segments(F, rx, ry, L.sa, L.sb, L.sk);
     int n = 0;
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
-        sk[i] = sk[i] && want;
-        n += sk[i];
+        L.sk[i] = L.sk[i] && want;
+        n += L.sk[i];
     }
     int incl = n;  // inclusive warp scan of the counts
 #pragma unroll
@@ -468,16 +472,26 @@ __device__ __forceinline__ int aniso_gather(const AnisoFoot& F, bool want, int r
         const int t = __shfl_up_sync(mask, incl, o);
         if (lane >= o) incl += t;
     }
-    int j = incl - n;
-    const int tag = lane | (F.minu << 5);
+    L.base = incl - n;
+    L.total = __shfl_sync(mask, incl, 31);
+}
+
+// Writes the segments r0 .. r0 + kAnisoSegs - 1 of the warp's list (those of this lane among them) to the
+// warp's shared memory.  The segments are then spread over the warp's lanes: a warp typically has a handful
+// of footprints of four segments each, so integrating each footprint on its own lane leaves most lanes idle
+// behind the longest boundary.  (Cutting the segments further into chunks of a few cells, to fill all 32
+// lanes, measured slower: 5-27 %.)
+__device__ __forceinline__ void aniso_put(const SegList& L, int r0, const AnisoWarp& W, int tag) {
+    int j = L.base - r0;
 #pragma unroll
     for (int i = 0; i < 5; ++i)
-        if (sk[i]) {
-            W.seg[j] = make_float4(sa[i].x, sa[i].y, sb[i].x, sb[i].y);
-            W.own[j] = tag;
+        if (L.sk[i]) {
+            if (j >= 0 && j < kAnisoSegs) {
+                W.seg[j] = make_float4(L.sa[i].x, L.sa[i].y, L.sb[i].x, L.sb[i].y);
+                W.own[j] = tag;
+            }
             ++j;
         }
-    return __shfl_sync(mask, incl, 31);
 }
 
 // Every lane's footprint integral (before the division by the area) for the lanes with want set, the warp's
@@ -488,23 +502,29 @@ __device__ __forceinline__ float4 aniso_boundary_sum(const AnisoFoot& F, bool wa
                                                      const AnisoWarp& W, unsigned mask) {
     const int lane = threadIdx.x & 31;
     want = want && F.maxu > F.minu && F.maxv > F.minv;  // no cell (also: rx or ry below 2): nothing to walk
-    const int n = aniso_gather(F, want, rx, ry, W, mask);
+    if (!__any_sync(mask, want)) return make_float4(0.f, 0.f, 0.f, 0.f);  // (the adjoint reading records)
+    SegList L;
+    aniso_segments(F, want, rx, ry, mask, L);
     W.lane[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
-    __syncwarp(mask);
-    for (int t = lane; t < n; t += 32) {
-        const float4 sg = W.seg[t];
-        const int ow = W.own[t];
-        const float2 a = make_float2(sg.x, sg.y), b = make_float2(sg.z, sg.w);
-        float4 r;
-        if constexpr (kShared) r = segment_sum_shared<Tex>(a, b, ow >> 5, textures, tex_base, P, rx, ry, scale);
-        else r = segment_sum<Tex>(a, b, ow >> 5, textures, tex_base, P, rx, ry, scale);
-        float* dst = reinterpret_cast<float*>(W.lane + (ow & 31));
-        atomicAdd(dst, r.x);
-        atomicAdd(dst + 1, r.y);
-        atomicAdd(dst + 2, r.z);
-        atomicAdd(dst + 3, r.w);
+    for (int r0 = 0; r0 < L.total; r0 += kAnisoSegs) {
+        aniso_put(L, r0, W, lane | (F.minu << 5));
+        __syncwarp(mask);
+        const int n = min(kAnisoSegs, L.total - r0);
+        for (int t = lane; t < n; t += 32) {
+            const float4 sg = W.seg[t];
+            const int ow = W.own[t];
+            const float2 a = make_float2(sg.x, sg.y), b = make_float2(sg.z, sg.w);
+            float4 r;
+            if constexpr (kShared) r = segment_sum_shared<Tex>(a, b, ow >> 5, textures, tex_base, P, rx, ry, scale);
+            else r = segment_sum<Tex>(a, b, ow >> 5, textures, tex_base, P, rx, ry, scale);
+            float* dst = reinterpret_cast<float*>(W.lane + (ow & 31));
+            atomicAdd(dst, r.x);
+            atomicAdd(dst + 1, r.y);
+            atomicAdd(dst + 2, r.z);
+            atomicAdd(dst + 3, r.w);
+        }
+        __syncwarp(mask);  // the list is read before the next round rewrites it
     }
-    __syncwarp(mask);
     const float4 r = W.lane[lane];
     __syncwarp(mask);  // read before the next call reuses the slots
     return r;
@@ -516,14 +536,21 @@ __device__ __forceinline__ void aniso_boundary_scatter(const AnisoFoot& F, float
                                                        int rx, int ry, const AnisoWarp& W, unsigned mask) {
     const int lane = threadIdx.x & 31;
     want = want && F.maxu > F.minu && F.maxv > F.minv;
-    const int n = aniso_gather(F, want, rx, ry, W, mask);
+    if (!__any_sync(mask, want)) return;
+    SegList L;
+    aniso_segments(F, want, rx, ry, mask, L);
     W.lane[lane] = g;
-    __syncwarp(mask);
-    for (int t = lane; t < n; t += 32) {
-        const float4 sg = W.seg[t];
-        segment_scatter(make_float2(sg.x, sg.y), make_float2(sg.z, sg.w), W.lane[W.own[t] & 31], vt, vP, rx, ry);
+    for (int r0 = 0; r0 < L.total; r0 += kAnisoSegs) {
+        aniso_put(L, r0, W, lane);
+        __syncwarp(mask);
+        const int n = min(kAnisoSegs, L.total - r0);
+        for (int t = lane; t < n; t += 32) {
+            const float4 sg = W.seg[t];
+            segment_scatter(make_float2(sg.x, sg.y), make_float2(sg.z, sg.w), W.lane[W.own[t] & 31], vt, vP, rx,
+                            ry);
+        }
+        __syncwarp(mask);  // the list is read before the next round rewrites it
     }
-    __syncwarp(mask);  // done with the slots before the next call reuses them
 }
 
 // Bilinear weights of a cell's four texels (u,v), (u+1,v), (u,v+1), (u+1,v+1) from its moments.
