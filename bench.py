@@ -351,13 +351,15 @@ def _run_ours(args, rank, world, local, dev):
         f_tile = min(tile, 16)
         f_steps = min(args.steps, 5)
         for filt in ("mipmapped2", "anisotropic_bilinear"):
-            total_f, per_f, stages_f, _, out_f = timed(store, f_tile, False, f_steps, args.warmup,
-                                                       depth if f_tile == tile else 0, filt)
+            # anisotropic_bilinear at its own default batch depth (ANISO_BATCH_DEPTH)
+            f_depth = depth if f_tile == tile and filt != "anisotropic_bilinear" else 0
+            total_f, per_f, stages_f, _, out_f = timed(store, f_tile, False, f_steps, args.warmup, f_depth, filt)
             del out_f
             total_f = max_over_ranks(total_f, world)
             filters[filt] = {
                 "value": round(C * H * W * world * f_steps / (total_f / 1e3) / 1e6, 2), "unit": "Mpix/s",
                 "ms_per_step": round(total_f / f_steps, 3), "steps": f_steps, "tile_size": f_tile,
+                "batch_depth": f_depth or "default",
                 "per_step_ms": [round(x, 3) for x in per_f],
                 "allocator_segments_in_timed_steps": timed_info["segments_allocated"],
                 "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stages_f.items()}}
