@@ -12,7 +12,10 @@ cameras, tile 8 -- against the oracle where it can follow at this size:
     FP32 storage: colours and alphas to 1e-5 with the 1e-3 flip budget,
     gradients to 1e-4 relative L2 (or 1.5x the IEEE-FP32 oracle's own error
     where that is larger).  Every form: render PSNR and gradient cosine are
-    printed; BF16 and FP16 must reach 50 dB and 0.999, FP8 35 dB and 0.99.
+    printed; BF16 and FP16 must reach 50 dB and 0.999, FP8 35 dB and 0.99;
+  * the anisotropic_bilinear filter (FP32 storage) on the same sampled tiles,
+    against the oracle's cell-by-cell footprint integration, at the FP32
+    tolerances above.
 """
 import numpy as np
 import pytest
@@ -142,3 +145,53 @@ def test_mixture1m_storage_forms_on_sampled_tiles(mixture, sampled_oracle, fmt):
         floor_db, floor_cos = (35.0, 0.99) if fmt == "fp8" else (50.0, 0.999)
         assert psnr >= floor_db, psnr
         assert min(cos.values()) >= floor_cos, cos
+
+
+@pytest.fixture(scope="module")
+def sampled_oracle_aniso(mixture, sampled_oracle):
+    """The FP64 and IEEE-FP32 oracle of the anisotropic_bilinear filter on the same sampled tiles."""
+    d, o = mixture, sampled_oracle
+    C, N, W, H, tw, th = d["C"], d["N"], d["W"], d["H"], d["tw"], d["th"]
+    mask = np.zeros((C, th, tw), np.uint8)
+    mask[:, ROW, ::10] = 1
+    rows = o["rows"]
+    remap = np.zeros(N, np.int64)
+    remap[rows] = np.arange(rows.size)
+    gid = remap[np.arange(C * N) % N]
+    tex_sub = d["tex"][T(rows, torch.int64)].cpu().numpy()
+    args = (to_np(d["means2d"]), to_np(d["M"]), to_np(d["colors"]), d["opac"], to_np(d["normals"]), tex_sub,
+            d["off"].cpu().numpy(), d["fl"].cpu().numpy(), W, H, TILE)
+    z3, z1 = np.zeros((C, H, W, 3), np.float32), np.zeros((C, H, W, 1), np.float32)
+    out = {}
+    for dt in (np.float64, np.float32):
+        kw = dict(masks=mask, gaussian_ids=gid, n_gauss=rows.size, aniso=True, dtype=dt)
+        fo = O.raster_fwd(*args, **kw)
+        out[dt] = (fo, O.raster_bwd(*args, fo, o["up_c"], o["up_a"], z3, z1, z1, mode=0, **kw))
+    return out
+
+
+def test_mixture1m_anisotropic_bilinear_on_sampled_tiles(mixture, sampled_oracle, sampled_oracle_aniso):
+    """The anisotropic_bilinear filter at full size (boundary integration, forward integral records, prefix
+    fold), FP32 texture storage, against the FP64 oracle's cell-by-cell integration on the sampled tiles."""
+    d, o = mixture, sampled_oracle
+    m2d = d["means2d"].detach().clone().requires_grad_()
+    M = d["M"].detach().clone().requires_grad_()
+    cols = d["colors"].detach().clone().requires_grad_()
+    op = T(d["opac"]).requires_grad_()
+    tex = d["tex"].detach().requires_grad_()
+    out = rasterize_to_pixels_textured_gaussians(
+        m2d, M, cols, op, tex, 3.0, 3.0, d["normals"], torch.zeros_like(m2d), d["W"], d["H"], TILE, d["off"],
+        d["fl"], filtering="anisotropic_bilinear")
+    ((out[0] * T(o["up_c"])).sum() + (out[1] * T(o["up_a"])).sum()).backward()
+    (fo, ob), (_, ob32) = sampled_oracle_aniso[np.float64], sampled_oracle_aniso[np.float32]
+    sel = o["sel"]
+    assert_close(to_np(out[0])[sel], fo.colors[sel], 1e-5, 1e-5, 1e-3, "colors")
+    assert_close(to_np(out[1])[sel], fo.alphas[sel], 1e-5, 0.0, 1e-3, "alphas")
+    grads = [("means2d", m2d.grad, ob.v_means2d, ob32.v_means2d), ("M", M.grad, ob.v_M, ob32.v_M),
+             ("colors", cols.grad, ob.v_colors, ob32.v_colors),
+             ("opacities", op.grad, ob.v_opacities, ob32.v_opacities),
+             ("textures", tex.grad[T(o["rows"], torch.int64)], ob.v_textures, ob32.v_textures)]
+    for k, g, ref, ref32 in grads:
+        assert np.abs(ref).max() > 0, k
+        bound = max(1e-4, 1.5 * rel_l2(ref32, ref))
+        assert rel_l2(to_np(g), ref) < bound, (k, rel_l2(to_np(g), ref), bound)
