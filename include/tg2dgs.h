@@ -403,7 +403,8 @@ typedef struct {
     /* TG_FILTER_ANISO_BILINEAR: the anisotropic_bilinear filter
      * (rasterize_to_pixels_aniso_bilinear_textured_gaussians_2dgs_{fwd,bwd}.cu
      * of the reference): each pixel's footprint quad in texel space integrates
-     * the bilinear interpolant cell by cell.  Same support as mipmapped2
+     * the bilinear interpolant (cell by cell, or along the footprint's boundary
+     * when aniso_prefix is given).  Same support as mipmapped2
      * (F32 / BF16 storage, 3 or 4 channels, tile 8 or 16, one CTA per tile,
      * reference adjoint). */
     int32_t filter;
