@@ -26,7 +26,10 @@ defined), and writes ``tests/golden/ref_<case>.npz``:
            the sampled tiles' splat lists and the projected rows they use;
   mix1m    camera 0 of the benchmark workload (bench.py's make_scene and
            gpu_textures: 1,000,000 splats, 32x32 FP32 textures drawn on the
-           GPU, 1600x1200, tile 8), sampled the same way.
+           GPU, 1600x1200, tile 8), sampled the same way;
+  mix1m_aniso  the same camera and textures with the anisotropic_bilinear
+           compositor, on other sampled tile rows, the splat lists keeping
+           only the rows whose footprints stay convex (aniso_safe_rows).
 
 For views8 and mix1m the reference's compositor runs on the sampled tiles'
 sub-problem (see sampled_case): with the whole texture tensor it refuses the
@@ -297,14 +300,15 @@ def subset(s, rows):
     return t
 
 
-def sampled_case(W, s, tex, sample_rows, every, seed):
+def sampled_case(W, s, tex, sample_rows, every, seed, filtering="bilinear", safe_rows=None):
     """Camera 0 of a large scene; outputs on sampled tiles, upstream gradients only there.
 
     The reference projects, shades and intersects the whole scene.  Its compositor cannot take the
     whole texture tensor (over 2^31 elements: it indexes textures through a 32-bit packed accessor and
     refuses the call), so it runs on the sampled tiles' sub-problem: the Gaussians their splat lists
     use, in ascending id order, and offsets that give every other tile an empty list.  A tile's result
-    depends only on its own list, so this is the reference's result for those tiles."""
+    depends only on its own list, so this is the reference's result for those tiles.  safe_rows (sorted
+    Gaussian ids): the splat lists keep only those (anisotropic_bilinear: the rows aniso_safe_rows allows)."""
     means, quats, scales, colors = T(s.means), T(s.quats), T(s.scales), T(s.colors)
     with torch.no_grad():
         p = project_and_shade(W, s, means, quats, scales, colors)
@@ -320,6 +324,8 @@ def sampled_case(W, s, tex, sample_rows, every, seed):
     fl = npy(p["flatten_ids"])
     tiles = np.flatnonzero(mask.reshape(-1))
     lists = [fl[off[t]:(off[t + 1] if t + 1 < off.size else fl.size)] for t in tiles]
+    if safe_rows is not None:
+        lists = [x[np.isin(x, safe_rows)] for x in lists]
     rows = np.unique(np.concatenate(lists))
     d = {"inputs_sha256": np.array(digest(s.means, s.quats, s.scales, s.opacities, s.colors, s.viewmats, s.Ks)),
          "up_seed": np.array(seed), "sample_rows": np.array(sample_rows), "sample_every": np.array(every),
@@ -335,19 +341,20 @@ def sampled_case(W, s, tex, sample_rows, every, seed):
     sub["offsets"] = T(sub_off, torch.int32)
     sub["flatten_ids"] = T(sub_fl, torch.int32)
     op_c = T(s.opacities[rows])[None].contiguous()
-    res = compositor(W, sub, s, sub_tex, op_c, "bilinear", ups)
+    res = compositor(W, sub, s, sub_tex, op_c, filtering, ups)
     for k in ("radii", "means2d", "depths", "M", "normals", "colors"):
         d[f"stage__{k}"] = npy(p[k])[0, rows]
     d["stage__n_isects"] = np.array(fl.size)
     d["stage__isect_digest"] = np.array(digest(npy(p["isect_ids"]), fl, off))
     sel = pix[..., 0] > 0
+    pre = f"comp_{filtering}"
     for i in range(5):
-        d[f"comp_bilinear__out{i}"] = res[f"out{i}"][sel]
+        d[f"{pre}__out{i}"] = res[f"out{i}"][sel]
     for k in ("means2d", "M", "colors", "opacities", "normals"):
-        d[f"comp_bilinear__v_{k}"] = res[f"v_{k}"][0]
+        d[f"{pre}__v_{k}"] = res[f"v_{k}"][0]
     keep, vals, norms = keep_rows(res["v_textures"], ROWS_KEPT_LARGE)
-    d["comp_bilinear__v_textures_rows"], d["comp_bilinear__v_textures_vals"] = keep, vals
-    d["comp_bilinear__v_textures_norms"] = norms
+    d[f"{pre}__v_textures_rows"], d[f"{pre}__v_textures_vals"] = keep, vals
+    d[f"{pre}__v_textures_norms"] = norms
     return d
 
 def main():
@@ -383,7 +390,7 @@ def main():
         del tex
         torch.cuda.empty_cache()
         print("views8 done", flush=True)
-    if "mix1m" in cases:
+    if "mix1m" in cases or "mix1m_aniso" in cases:
         import bench
 
         sc = bench.make_scene(0, 1, 1_000_000, 4)
@@ -391,9 +398,14 @@ def main():
                          sc["viewmats"][:1], sc["Ks"][:1], sc["width"], sc["height"], 0, far_plane=100.0,
                          tile_size=8, name="mix1m")
         tex = bench.gpu_textures(s.means.shape[0], 32, torch.device(DEV))
-        d = sampled_case(W, s, tex, (60, 95), 10, 303)
-        np.savez_compressed(os.path.join(a.out, "ref_mix1m.npz"), **d)
-        print("mix1m done", flush=True)
+        if "mix1m" in cases:
+            d = sampled_case(W, s, tex, (60, 95), 10, 303)
+            np.savez_compressed(os.path.join(a.out, "ref_mix1m.npz"), **d)
+            print("mix1m done", flush=True)
+        if "mix1m_aniso" in cases:
+            d = sampled_case(W, s, tex, (40, 75, 110), 10, 304, "anisotropic_bilinear", aniso_safe_rows(W, s))
+            np.savez_compressed(os.path.join(a.out, "ref_mix1m_aniso.npz"), **d)
+            print("mix1m_aniso done", flush=True)
 
 if __name__ == "__main__":
     main()

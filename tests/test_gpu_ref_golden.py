@@ -18,8 +18,9 @@ on identical inputs:
     two --use_fast_math builds); contribution sums 1e-4 relative;
   * compositor adjoint: every gradient within 1e-4 relative L2 per tensor
     (texture gradients on the stored rows, and every row's norm); for the
-    sampled large workloads, where pixels hold up to ~190 contributors and
-    both builds recover transmittance by division, 1e-3;
+    sampled large workloads (views8 and the benchmark scene's camera 0 with
+    bilinear, and with anisotropic_bilinear), where pixels hold up to ~190
+    contributors and both builds recover transmittance by division, 1e-3;
   * the renderer end to end (rasterization_textured_gaussians, the
     reference's public entry point) on the small workloads: images 1e-5 with
     the flip budget, leaf gradients 1e-4 relative L2 (1e-3 for mipmapped2 and
@@ -293,9 +294,13 @@ def _sampled_scene(case):
     return s, s.opacities, 8
 
 
-@pytest.mark.parametrize("case", ["views8", "mix1m"])
+@pytest.mark.parametrize("case", ["views8", "mix1m", "mix1m_aniso"])
 def test_compositor_matches_reference_on_sampled_tiles(case):
+    """mix1m_aniso: the anisotropic_bilinear filter (boundary integration, forward records, prefix fold) on
+    the benchmark scene's camera 0 against the reference's own cell-by-cell kernels."""
     g = RG.load(case)
+    filtering = "anisotropic_bilinear" if case.endswith("_aniso") else "bilinear"
+    pre = f"comp_{filtering}"
     s, opac, tile = _sampled_scene(case)
     N = s.means.shape[0]
     rows = g["rows"]
@@ -310,12 +315,12 @@ def test_compositor_matches_reference_on_sampled_tiles(case):
     densify = torch.zeros_like(leaves["means2d"], requires_grad=True)
     out = rasterize_to_pixels_textured_gaussians(
         leaves["means2d"], leaves["M"], leaves["colors"], leaves["opacities"], tex, 3.0, 3.0, leaves["normals"],
-        densify, W, H, tile, T(offsets, torch.int32), T(fl, torch.int32))
+        densify, W, H, tile, T(offsets, torch.int32), T(fl, torch.int32), filtering=filtering)
     sel = RG.pixel_mask(g, tile, th, tw, H, W)
     assert sel.sum() >= 2000
     problems, report = [], []
     for i, name in enumerate(("colors", "alphas", "normals", "distort", "median")):
-        a, b = to_np(out[i])[sel].astype(np.float64), g[f"comp_bilinear__out{i}"].astype(np.float64)
+        a, b = to_np(out[i])[sel].astype(np.float64), g[f"{pre}__out{i}"].astype(np.float64)
         err = np.abs(a - b)
         frac = float((err > 1e-5 + 1e-5 * np.abs(b)).mean())
         report.append(f"{name}: max {err.max():.2e}, frac>1e-5 {frac:.2e}")
@@ -324,8 +329,8 @@ def test_compositor_matches_reference_on_sampled_tiles(case):
     selt = T(sel.astype(np.float32)[..., None])
     ups = RG.upstream(g["up_seed"], s)
     sum((o * T(u) * selt).sum() for o, u in zip(out[:5], ups)).backward()
-    grads = [(k, to_np(v.grad)[0], g[f"comp_bilinear__v_{k}"]) for k, v in leaves.items()]
-    rows_k, vals, norms, ours = RG.texture_rows_check(g, "comp_bilinear", to_np(tex.grad))
+    grads = [(k, to_np(v.grad)[0], g[f"{pre}__v_{k}"]) for k, v in leaves.items()]
+    rows_k, vals, norms, ours = RG.texture_rows_check(g, pre, to_np(tex.grad))
     grads.append(("texture rows", ours, vals))
     mine = np.linalg.norm(to_np(tex.grad).reshape(rows.size, -1).astype(np.float64), axis=1)
     grads.append(("texture row norms", mine, norms))
