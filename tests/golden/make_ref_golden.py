@@ -27,8 +27,9 @@ defined), and writes ``tests/golden/ref_<case>.npz``:
   mix1m    camera 0 of the benchmark workload (bench.py's make_scene and
            gpu_textures: 1,000,000 splats, 32x32 FP32 textures drawn on the
            GPU, 1600x1200, tile 8), sampled the same way;
-  mix1m_mip  the same camera and textures with the mipmapped2 compositor, on
-           other sampled tile rows;
+  mix1m_bwd2, mix1m_mip  the same camera and textures with the bilinear_bwd2
+           adjoint and with the mipmapped2 compositor, on other sampled tile
+           rows;
   mix1m_aniso  the same camera and textures with the anisotropic_bilinear
            compositor, on other sampled tile rows, the splat lists keeping
            only the rows whose footprints stay convex (aniso_safe_rows).
@@ -392,7 +393,7 @@ def main():
         del tex
         torch.cuda.empty_cache()
         print("views8 done", flush=True)
-    if "mix1m" in cases or "mix1m_mip" in cases or "mix1m_aniso" in cases:
+    if any(c.startswith("mix1m") for c in cases):
         import bench
 
         sc = bench.make_scene(0, 1, 1_000_000, 4)
@@ -404,6 +405,10 @@ def main():
             d = sampled_case(W, s, tex, (60, 95), 10, 303)
             np.savez_compressed(os.path.join(a.out, "ref_mix1m.npz"), **d)
             print("mix1m done", flush=True)
+        if "mix1m_bwd2" in cases:
+            d = sampled_case(W, s, tex, (30, 120), 10, 306, "bilinear_bwd2")
+            np.savez_compressed(os.path.join(a.out, "ref_mix1m_bwd2.npz"), **d)
+            print("mix1m_bwd2 done", flush=True)
         if "mix1m_mip" in cases:
             d = sampled_case(W, s, tex, (50, 85), 10, 305, "mipmapped2")
             np.savez_compressed(os.path.join(a.out, "ref_mix1m_mip.npz"), **d)

@@ -19,7 +19,7 @@ on identical inputs:
   * compositor adjoint: every gradient within 1e-4 relative L2 per tensor
     (texture gradients on the stored rows, and every row's norm); for the
     sampled large workloads (views8 and the benchmark scene's camera 0 with
-    bilinear, mipmapped2 and anisotropic_bilinear), where pixels hold up to ~190
+    bilinear, bilinear_bwd2, mipmapped2 and anisotropic_bilinear), where pixels hold up to ~190
     contributors and both builds recover transmittance by division, 1e-3;
   * the renderer end to end (rasterization_textured_gaussians, the
     reference's public entry point) on the small workloads: images 1e-5 with
@@ -294,13 +294,14 @@ def _sampled_scene(case):
     return s, s.opacities, 8
 
 
-@pytest.mark.parametrize("case", ["views8", "mix1m", "mix1m_mip", "mix1m_aniso"])
+@pytest.mark.parametrize("case", ["views8", "mix1m", "mix1m_bwd2", "mix1m_mip", "mix1m_aniso"])
 def test_compositor_matches_reference_on_sampled_tiles(case):
-    """mix1m_mip / mix1m_aniso: the mipmapped2 and anisotropic_bilinear filters (the latter by boundary
-    integration, forward records and prefix fold) on the benchmark scene's camera 0 against the reference's
-    own kernels."""
+    """mix1m_bwd2 / _mip / _aniso: the bilinear_bwd2 adjoint, and the mipmapped2 and anisotropic_bilinear
+    filters (the latter by boundary integration, forward records and prefix fold) on the benchmark scene's
+    camera 0 against the reference's own kernels."""
     g = RG.load(case)
-    filtering = {"mix1m_mip": "mipmapped2", "mix1m_aniso": "anisotropic_bilinear"}.get(case, "bilinear")
+    filtering = {"mix1m_bwd2": "bilinear_bwd2", "mix1m_mip": "mipmapped2",
+                 "mix1m_aniso": "anisotropic_bilinear"}.get(case, "bilinear")
     pre = f"comp_{filtering}"
     s, opac, tile = _sampled_scene(case)
     N = s.means.shape[0]
