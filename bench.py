@@ -403,6 +403,40 @@ def _run_ours(args, rank, world, local, dev):
                   "bf16_one_call": {"value": round(pix_r * world / (ms_head / 1e3) / 1e6, 2), "unit": "Mpix/s",
                                     "ms_per_step": round(ms_head, 3),
                                     "form": f"BF16 storage, one call, tile {tile}, batch depth {depth or tile * tile}"}}
+        # the other filters on the same splats as the reference arm times them (anisotropic_bilinear on the
+        # splats whose footprints stay convex in every view): FP32 textures one call per camera, and BF16
+        # storage in one call
+        same_n["filters"] = {}
+        for filt in ("mipmapped2", "anisotropic_bilinear"):
+            n_f = reference_cuda_splats(N, R, filt)
+            scf, texf = sc_r, tex_r
+            if n_f != n_ref:
+                scf = make_scene(rank, world, n_f, C)
+                texf = gpu_textures(n_f, R, dev)
+            if filt == "anisotropic_bilinear":
+                keep = aniso_safe_subset(scf, dev)
+                scf = dict(scf, **{k: np.ascontiguousarray(scf[k][keep]) for k in
+                                   ("means", "quats", "scales", "opacities", "colors")})
+                texf = gpu_textures(keep.size, R, dev)
+            storef, _ = make_texture_storage(texf.detach(), "bf16")
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            f_tile = min(tile, 16)
+            f_depth = depth if f_tile == tile and filt != "anisotropic_bilinear" else 0
+            ms_p = max_over_ranks(time_renderer(rasterization_textured_gaussians, scf, texf, dev, 16, 3, 2, True,
+                                                filtering=filt), world)
+            ms_o = max_over_ranks(time_renderer(rasterization_textured_gaussians, scf, texf, dev, f_tile, 3, 2,
+                                                False, filtering=filt, texture_storage=storef, batch_depth=f_depth,
+                                                tile_order=args.tile_order), world)
+            same_n["filters"][filt] = {
+                "splats": int(scf["means"].shape[0]),
+                "fp32_per_camera": {"value": round(pix_r * world / (ms_p / 1e3) / 1e6, 2), "unit": "Mpix/s",
+                                    "ms_per_step": round(ms_p, 3), "form": "FP32 textures, one call per camera, tile 16"},
+                "bf16_one_call": {"value": round(pix_r * world / (ms_o / 1e3) / 1e6, 2), "unit": "Mpix/s",
+                                  "ms_per_step": round(ms_o, 3), "form": f"BF16 storage, one call, tile {f_tile}"}}
+            del storef
+            if texf is not tex_r:
+                del texf
         del tex_r, store_r
         torch.cuda.empty_cache()
 
@@ -922,8 +956,13 @@ def _run_batch(args, dev):
 # The reference indexes textures through 32-bit packed accessors and refuses a texture tensor of more than
 # 2^31 - 1 elements (1,000,000 x 32 x 32 x 4 is 4.2e9): its CUDA path is timed at the largest splat count in
 # steps of 100,000 that it accepts (500,000 at 32x32), and this arm's own form is timed there too.
-def reference_cuda_splats(n_splats: int, R: int) -> int:
-    cap = (2**31 - 1) // (R * R * 4)
+def reference_cuda_splats(n_splats: int, R: int, filtering: str = "bilinear") -> int:
+    """The most splats (in 100,000s) the reference's compositor takes: it refuses texture tensors of 2^31
+    elements or more -- for mipmapped2 its full pyramid, (4^(L+1) - 1) / 3 texels a splat."""
+    texels = R * R
+    if filtering == "mipmapped2":
+        texels = (4 * R * R - 1) // 3
+    cap = (2**31 - 1) // (texels * 4)
     return min(n_splats, cap // 100_000 * 100_000 if cap >= 100_000 else cap)
 
 
@@ -972,6 +1011,35 @@ def time_renderer(render, sc, tex, dev, tile, steps, warmup, per_view, **kw):
     return timed_plain(step, steps, warmup)
 
 
+def aniso_safe_subset(sc, dev, tile=16):
+    """Indices of the splats whose footprint quads stay convex on every pixel of every tile they touch, in
+    every view.  The reference's anisotropic_bilinear clipping keeps at most 8 vertices in fixed arrays
+    (filters/anisotropic_bilinear.cuh:80-160); a pixel whose corner rays meet the splat's plane on both
+    sides gives a self-intersecting quad that can need more (undefined behaviour), so its timing runs only
+    on splats that stay 1.5 (radius + tile + 2) pixels from that line, z(px, py) = 0, in all views."""
+    import torch
+
+    from textured_gaussians_b200.cuda import fully_fused_projection_2dgs
+
+    T = lambda x: torch.from_numpy(x).to(dev)
+    with torch.no_grad():
+        radii, m2d, _, M, _ = fully_fused_projection_2dgs(
+            T(sc["means"]), T(sc["quats"]), T(sc["scales"]), T(sc["viewmats"]), T(sc["Ks"]), sc["width"],
+            sc["height"], 0.3, 0.01, 100.0, 0.0)
+    r = radii.cpu().numpy().astype(np.float64)
+    M = M.cpu().numpy().astype(np.float64)
+    c = m2d.cpu().numpy().astype(np.float64)
+    M0, M1, M2 = M[..., 0, :], M[..., 1, :], M[..., 2, :]
+
+    def cz(u, v):
+        return u[..., 0] * v[..., 1] - u[..., 1] * v[..., 0]
+
+    a, b, c0 = -cz(M2, M1), -cz(M0, M2), cz(M0, M1)
+    dist = np.abs(a * c[..., 0] + b * c[..., 1] + c0) / np.maximum(np.hypot(a, b), 1e-300)
+    keep = ((r <= 0) | (dist >= 1.5 * (r + tile + 2))).all(axis=0)
+    return np.flatnonzero(keep)
+
+
 def reference_cuda(args):
     """The reference's own CUDA path on this GPU: its renderer, FP32 textures, one call per camera (the only
     defined form), at reference_cuda_splats() splats; None where its build or install is absent."""
@@ -994,6 +1062,30 @@ def reference_cuda(args):
         tex = gpu_textures(n, R, dev)
         ms = time_renderer(ref.rasterization_textured_gaussians, sc, tex, dev, tile, 5, 2, True)
         out[f"tile{tile}"] = {"value": round(pix / (ms / 1e3) / 1e6, 2), "unit": "Mpix/s", "ms_per_step": round(ms, 3)}
+        del tex
+        torch.cuda.empty_cache()
+    # the other texture filters, same form: mipmapped2 (a zero background: its adjoint returns a background
+    # gradient for a None background, which autograd rejects) and anisotropic_bilinear on the splats whose
+    # footprints stay convex in every view (aniso_safe_subset)
+    out["filters"] = {}
+    bg = torch.zeros((1, 3), device=dev)
+    for filt in ("mipmapped2", "anisotropic_bilinear"):
+        nf = reference_cuda_splats(args.splats, R, filt)
+        scf = sc if nf == n else make_scene(0, 1, nf, args.cameras)
+        if filt == "anisotropic_bilinear":
+            keep = aniso_safe_subset(sc, dev)
+            scf = dict(scf, **{k: np.ascontiguousarray(scf[k][keep]) for k in
+                               ("means", "quats", "scales", "opacities", "colors")})
+        nf = scf["means"].shape[0]
+        tex = gpu_textures(nf, R, dev)
+        steps, warm = (2, 1) if filt == "anisotropic_bilinear" else (5, 2)
+        res = {"splats": nf}
+        for tile in ((16,) if filt == "anisotropic_bilinear" else (16, 8)):  # bounded: about 1 s a step
+            ms = time_renderer(ref.rasterization_textured_gaussians, scf, tex, dev, tile, steps, warm, True,
+                               filtering=filt, backgrounds=bg)
+            res[f"tile{tile}"] = {"value": round(pix / (ms / 1e3) / 1e6, 2), "unit": "Mpix/s",
+                                  "ms_per_step": round(ms, 3)}
+        out["filters"][filt] = res
         del tex
         torch.cuda.empty_cache()
     return out
