@@ -619,8 +619,10 @@ def generate_mipmap(textures: Tensor, log_texture_res: int, log_reduce: int = 4,
 # (every footprint cell by cell, as the reference does).  The same integral up to FP32 rounding.
 ANISO_INTEGRATION = "boundary"
 # Footprint integrals per pixel the forward keeps for the adjoint with the boundary integration (0: none;
-# the adjoint then integrates every footprint again).  Each pixel's first ANISO_RECORDS are kept.
+# the adjoint then integrates every footprint again).  Each pixel's first ANISO_RECORDS are kept, within
+# ANISO_RECORDS_BYTES of device memory for the call (fewer per pixel on very large calls).
 ANISO_RECORDS = 32
+ANISO_RECORDS_BYTES = 8 << 30
 # Splats staged per compositor batch for the anisotropic_bilinear filter when the caller leaves batch_depth at
 # 0: its per-pair work dwarfs the staging, and a small batch leaves more of the L1 to the boundary walk's
 # texture reads (1M splats x four 1600x1200 views, tile 8: 382 ms per step at 32, 391 at 64).
@@ -722,11 +724,12 @@ class _RasterizeToPixelsTextured(torch.autograd.Function):
         a.aniso_prefix = B.ptr(prefix)
         # the footprint integrals, kept for the adjoint (which then need not integrate them again)
         records = counts = None
-        if prefix is not None and ANISO_RECORDS > 0 and any(ctx.needs_input_grad):
-            n_pix = math.prod(pshape)
-            records = torch.empty((n_pix, ANISO_RECORDS, 4), dtype=torch.float32, device=dev)
+        n_pix = math.prod(pshape)
+        cap = min(ANISO_RECORDS, ANISO_RECORDS_BYTES // max(1, 16 * n_pix))
+        if prefix is not None and cap > 0 and any(ctx.needs_input_grad):
+            records = torch.empty((n_pix, cap, 4), dtype=torch.float32, device=dev)
             counts = torch.empty((n_pix,), dtype=torch.int32, device=dev)
-            a.aniso_records, a.aniso_record_count, a.aniso_record_cap = B.ptr(records), B.ptr(counts), ANISO_RECORDS
+            a.aniso_records, a.aniso_record_count, a.aniso_record_cap = B.ptr(records), B.ptr(counts), cap
         B.call("tg_rasterize_fwd", st, B.lib().tg_rasterize_fwd, ctypes.byref(a), st)
         ctx.save_for_backward(means2d, ray_transforms, colors, opacities, textures, normals, densify, backgrounds, m,
                               tex_store, tex_scales, isect_offsets, flatten_ids, render_colors, render_alphas,
