@@ -236,3 +236,25 @@ def test_aniso_adjoint_from_forward_records_matches_integrating_again(name, inte
         for k, (got, ref) in enumerate(zip(grads[cap], grads[0])):
             assert np.abs(ref).max() > 0
             assert rel_l2(got, ref) < 1e-6, (cap, k, rel_l2(got, ref))
+
+
+def test_aniso_transmittance_checkpoints_match_division(integration):
+    """The adjoint restarting its transmittance from the forward's checkpoints (with the boundary form's
+    records and prefix fold, or cell by cell) against recovering it by division alone."""
+    s = SCENES["small"]()
+    d = _inputs(s, 8)
+    rng = np.random.default_rng(9)
+    up = T(rng.normal(size=(d["C"], s.height, s.width, 3)).astype(np.float32))
+    grads = {}
+    for mode in ("divide", "checkpoint"):
+        leaves = [d["means2d"].detach().clone().requires_grad_(), d["M"].detach().clone().requires_grad_(),
+                  T(d["opac"]).requires_grad_(), d["tex"].detach().clone().requires_grad_()]
+        out = rasterize_to_pixels_textured_gaussians(
+            leaves[0], leaves[1], T(d["colors"]), leaves[2], leaves[3], 3.0, 3.0, d["normals"],
+            torch.zeros_like(d["means2d"]), s.width, s.height, 8, d["off"], d["fl"], filtering="anisotropic_bilinear",
+            transmittance=mode)
+        (out[0] * up).sum().backward()
+        grads[mode] = [to_np(x.grad) for x in leaves]
+    for k, (a, b) in enumerate(zip(grads["checkpoint"], grads["divide"])):
+        assert np.abs(b).max() > 0
+        assert rel_l2(a, b) < 1e-4, (k, rel_l2(a, b))
