@@ -202,7 +202,7 @@ __device__ __forceinline__ void accumulate_pair(const tg_raster_bwd_args& a, con
             }
         }
     }
-    if (!Filt::kMip && !Filt::kAniso && kTextured && e.tex_valid && uv_scale != 0.f) {
+    if constexpr (Filt::kUV) if (kTextured && e.tex_valid && uv_scale != 0.f) {
         const float wu = e.w[1] + e.w[3], wv = e.w[2] + e.w[3];
         const float dbu[4] = {-(1.f - wv), 1.f - wv, -wv, wv};
         const float dbv[4] = {-(1.f - wu), -wu, 1.f - wu, wu};
@@ -520,6 +520,27 @@ void launch_filter_bwd(dim3 g, dim3 b, size_t smem, cudaStream_t s, const tg_ras
         raster_bwd_kernel<D, Tex, 1, false, Filt><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
 }
 
+// The bilinear adjoint instances: 32x32 tiles (four pixels per thread) or not, persistent or not.
+template <int D, class Tex, class F>
+const void* bilinear_bwd_fn(bool four, bool pers) {
+    if constexpr (F::kUV && Tex::kFormat == TG_TEX_NONE) return nullptr;  // (never asked for)
+    else
+        return four ? (pers ? (const void*)raster_bwd_kernel<D, Tex, 4, true, F>
+                            : (const void*)raster_bwd_kernel<D, Tex, 4, false, F>)
+                    : (pers ? (const void*)raster_bwd_kernel<D, Tex, 1, true, F>
+                            : (const void*)raster_bwd_kernel<D, Tex, 1, false, F>);
+}
+template <int D, class Tex, class F>
+void launch_bilinear_bwd(bool four, bool pers, dim3 g, dim3 b, size_t smem, cudaStream_t s,
+                         const tg_raster_bwd_args& a, float uv_scale, int bs, int64_t blocks) {
+    if constexpr (!(F::kUV && Tex::kFormat == TG_TEX_NONE)) {
+        if (four && pers) raster_bwd_kernel<D, Tex, 4, true, F><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        else if (four) raster_bwd_kernel<D, Tex, 4, false, F><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        else if (pers) raster_bwd_kernel<D, Tex, 1, true, F><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        else raster_bwd_kernel<D, Tex, 1, false, F><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+    }
+}
+
 template <int D, class Tex>
 cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     const tg_raster_fwd_args& f = a.f;
@@ -534,12 +555,12 @@ cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
     if ((mip || aniso) && !filter_instance<D, Tex, FiltMip2>()) return cudaErrorInvalidValue;
     const bool four = tile_px > 256;  // 32x32 tiles: four pixels per thread, 256 threads
     const bool pers = f.work_queue != nullptr;
+    // the bwd2 / exact adjoints (uv_scale != 0) take the instances that carry the UV term
+    const bool uv = Tex::kFormat != TG_TEX_NONE && uv_scale != 0.f;
     const void* fn = mip ? filter_bwd_fn<D, Tex, FiltMip2>()
                    : aniso ? filter_bwd_fn<D, Tex, FiltAniso>()
-                   : four ? (pers ? (const void*)raster_bwd_kernel<D, Tex, 4, true>
-                                  : (const void*)raster_bwd_kernel<D, Tex, 4, false>)
-                          : (pers ? (const void*)raster_bwd_kernel<D, Tex, 1, true>
-                                  : (const void*)raster_bwd_kernel<D, Tex, 1, false>);
+                   : uv ? bilinear_bwd_fn<D, Tex, FiltBilinearUV>(four, pers)
+                        : bilinear_bwd_fn<D, Tex, FiltBilinear>(four, pers);
     const int threads = four ? tile_px / 4 : tile_px;
     cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
@@ -552,10 +573,8 @@ cudaError_t launch_bwd_t(const tg_raster_bwd_args& a, cudaStream_t s) {
         const dim3 g((unsigned)grid), b((unsigned)threads);
         if (mip) launch_filter_bwd<D, Tex, FiltMip2>(g, b, smem, s, a, uv_scale, bs, blocks);
         else if (aniso) launch_filter_bwd<D, Tex, FiltAniso>(g, b, smem, s, a, uv_scale, bs, blocks);
-        else if (four && pers) raster_bwd_kernel<D, Tex, 4, true><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
-        else if (four) raster_bwd_kernel<D, Tex, 4, false><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
-        else if (pers) raster_bwd_kernel<D, Tex, 1, true><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
-        else raster_bwd_kernel<D, Tex, 1, false><<<g, b, smem, s>>>(a, uv_scale, bs, blocks);
+        else if (uv) launch_bilinear_bwd<D, Tex, FiltBilinearUV>(four, pers, g, b, smem, s, a, uv_scale, bs, blocks);
+        else launch_bilinear_bwd<D, Tex, FiltBilinear>(four, pers, g, b, smem, s, a, uv_scale, bs, blocks);
         note_launches(1);
     }
     if ((err = cudaGetLastError()) != cudaSuccess) return err;

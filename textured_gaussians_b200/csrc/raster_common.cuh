@@ -21,20 +21,28 @@ constexpr float kFilterInvSquare = 2.0f;
 // level, filters/mip2.cuh:27-105 of the reference) and anisotropic_bilinear
 // (the bilinear interpolant integrated over the pixel's footprint quad,
 // filters/anisotropic_bilinear.cuh:15-400: a variable number of texel cells).
+// kUV: the adjoint carries the texture lookup's dependence on the UV point (the bwd2 and exact adjoints); a
+// compile-time property so that the reference adjoint does not keep the taps live for it.
 struct FiltBilinear {
     static constexpr int kTaps = 4;
     static constexpr bool kMip = false;
     static constexpr bool kAniso = false;
+    static constexpr bool kUV = false;
+};
+struct FiltBilinearUV : FiltBilinear {
+    static constexpr bool kUV = true;
 };
 struct FiltMip2 {
     static constexpr int kTaps = 8;
     static constexpr bool kMip = true;
     static constexpr bool kAniso = false;
+    static constexpr bool kUV = false;
 };
 struct FiltAniso {
     static constexpr int kTaps = 1;  // unused: the footprint replaces the tap list
     static constexpr bool kMip = false;
     static constexpr bool kAniso = true;
+    static constexpr bool kUV = false;
 };
 
 template <int NT>
